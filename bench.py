@@ -1,0 +1,395 @@
+"""Benchmark of the B200 ECL-MST engine.
+
+One "step" is one complete minimum-spanning-forest solve of the workload
+graph (threshold choice, both scans, all Boruvka rounds), the reference's
+timed window (ECL-MST/ECL_MST.cu:301-345). The default workload is the
+single-graph configuration: RMAT scale 22, edge factor 16,
+(a,b,c) = (0.57, 0.19, 0.19), seed 2, int32 weights uniform in [1, 2^24],
+deduplicated and symmetrised (128,309,062 directed CSR entries), generated
+here from the seed (synthetic stand-in for the reference's downloaded
+inputs). Metric: Gedges/s = directed CSR entries / step time / 1e9, the
+artifact's throughput definition (generate_compare_tables.py:59) in G.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU implementation of the path,
+cpuMST (serial Kruskal, ECL_MST.cu:82-124) compiled from the reference
+sources (oracle/_ref), on a bounded sample of the workload.
+
+With N > 1 (torchrun) each rank solves its own replica of the graph on its
+GPU (a single graph does not shard: "replicas only"); value = all ranks'
+entries / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "mst-artifact-sc23_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "Gedges/s & graphs/s on 1 B200: learned/batched vs plain ECL-MST, exact inMST"
+RMAT = dict(a=0.57, b=0.19, c=0.19)
+WORKLOADS = {
+    # name: (generator kwargs, description)
+    "rmat22": ("rmat", dict(scale=22, edge_factor=16, seed=2, wmax=1 << 24),
+               "RMAT scale 22, ef 16, a=.57 b=.19 c=.19, seed 2, w~U[1,2^24]"),
+    "grid1000": ("grid", dict(rows=1000, cols=1000, seed=1, wmax=1_000_000),
+                 "2D 4-neighbour grid 1000x1000, seed 1, w~U[1,1e6]"),
+    "rmat25": ("rmat", dict(scale=25, edge_factor=16, seed=3, wmax=1 << 30),
+               "RMAT scale 25, ef 16, a=.57 b=.19 c=.19, seed 3, w~U[1,2^30]"),
+    "er16m": ("er", dict(nodes=1 << 24, avg_degree=32, seed=3, wmax=1 << 30),
+              "Erdos-Renyi 16,777,216 vertices, avg degree 32, seed 3, w~U[1,2^30]"),
+}
+CPU_SAMPLE = {"rmat22": ("rmat", dict(scale=20, edge_factor=16, seed=2, wmax=1 << 24),
+                         "RMAT scale 20 (same family and parameters, 1/4 of the entries)")}
+
+
+def make_graph(E, kind, kw):
+    if kind == "rmat":
+        return E.gen_rmat(kw["scale"], kw["edge_factor"], RMAT["a"], RMAT["b"], RMAT["c"], kw["seed"],
+                          kw["wmax"])
+    if kind == "grid":
+        return E.gen_grid(kw["rows"], kw["cols"], kw["seed"], kw["wmax"])
+    if kind == "er":
+        return E.gen_er(kw["nodes"], kw["avg_degree"], kw["seed"], kw["wmax"])
+    raise ValueError(kind)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or not self.path:
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, val in zip(names, parts[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def round_kernel_bytes(st, entry_bytes=16, atomics=None):
+    """Algorithmic bytes of the round kernels of one solve.
+
+    Per round with W_in entries in and W_out kept (both phases):
+      find/min pass:  S*W_in (read) + 2*4*W_in (parent, depth 1) + 2*8*W_in (guard reads)
+                      + S*W_out (compacted write) + 2*8*A (atomicMin)
+                      + 2*8*W_in (reset of the previous round's slots, rounds > 0)
+      mark pass:      S*W_out (read) + 2*8*W_out (min-slot reads)
+    A = guarded atomics actually issued when counted, else 2*W_out (upper bound).
+    """
+    total = 0
+    for p in range(2):
+        w = st["wl_in"][p]
+        for r in range(st["rounds"][p]):
+            win = w[r]
+            wout = w[r + 1] if r + 1 < len(w) else 0
+            total += entry_bytes * win + 8 * win + 16 * win + entry_bytes * wout
+            total += 16 * wout + entry_bytes * wout
+            if r > 0:
+                total += 16 * win
+    a = atomics if atomics is not None else 2 * sum(
+        (st["wl_in"][p][r + 1] if r + 1 < len(st["wl_in"][p]) else 0)
+        for p in range(2) for r in range(st["rounds"][p]))
+    total += 16 * a
+    return total
+
+
+def scan_kernel_bytes(st, nodes, edges, entry_bytes=16):
+    """Light scan: nindex + nlist + eweight + init of parent/min slots + appended entries.
+    Heavy scan: flatten (parent read+write) + nindex + nlist + eweight + appended."""
+    b = 4 * (nodes + 1) + 8 * edges + 20 * nodes + entry_bytes * st["scan_kept"][0]
+    if st["filtered"]:
+        b += 8 * nodes + 4 * (nodes + 1) + 8 * edges + entry_bytes * st["scan_kept"][1]
+    return b
+
+
+def reference_arm(args, E):
+    """bench.py --impl reference: the reference's cpuMST on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+
+    kind, kw, desc = CPU_SAMPLE.get(args.workload, WORKLOADS[args.workload])
+    g = make_graph(E, kind, kw)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        O.ref_cpu_mst(g.nindex, g.nlist, g.eweight)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    tot = sum(times)
+    value = args.steps * g.edges / tot / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Gedges/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32/uint64", "data": "synthetic",
+        "config": {"workload": args.workload, "sample": desc, "nodes": g.nodes, "edges": g.edges},
+        "cpu_baseline": {"value": value, "unit": "Gedges/s", "cores": 1, "kind": "reference",
+                         "sample": f"reference cpuMST (serial Kruskal, 1 thread) on {desc}"},
+        "e2e": {"value": value, "unit": "Gedges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat22")
+    ap.add_argument("--mode", choices=["heuristic", "learned", "quantile"], default="heuristic")
+    ap.add_argument("--quantile", type=float, default=0.1)
+    ap.add_argument("--split", type=int, default=0)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain ECL-MST comparison")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    import ecl_mst as E
+
+    if args.impl == "reference":
+        reference_arm(args, E)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    kind, kw, desc = WORKLOADS[args.workload]
+    t0 = time.perf_counter()
+    g = make_graph(E, kind, kw)
+    gen_s = time.perf_counter() - t0
+
+    mode = {"heuristic": E.THRESH_HEURISTIC, "learned": E.THRESH_LEARNED, "quantile": E.THRESH_QUANTILE}[args.mode]
+    opts = E.make_opts(mode=mode, quantile=args.quantile, degree_split=args.split)
+
+    ctx = E.Context(g.nodes, g.edges, device=local)
+    d_ni = torch.from_numpy(g.nindex).to(dev)
+    d_nl = torch.from_numpy(g.nlist).to(dev)
+    d_ew = torch.from_numpy(g.eweight).to(dev)
+    d_out = torch.empty(max(g.edges, 1), dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MB > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+
+    def solve(stats):
+        return ctx.run_device(g.nodes, g.edges, d_ni.data_ptr(), d_nl.data_ptr(), d_ew.data_ptr(),
+                              d_out.data_ptr(), opts=opts, stream=stream.cuda_stream, stats=stats)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        solve(True)
+    torch.cuda.synchronize()
+    # correctness of the timed configuration against the oracle-free invariant:
+    # forest weight is recomputed on the host from inMST below (exact check in tests)
+
+    step_ms, scan_ms, round_ms = [], [], []
+    last = None
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flush between timed iterations (outside the timed events)
+            st = solve(True)  # CUDA events around the solve on `stream`; syncs after
+            step_ms.append(st["ms_total"])
+            scan_ms.append(st["ms_scan"])
+            round_ms.append(st["ms_rounds"])
+            last = st
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = clk.summary()
+    ms_step = sum(step_ms) / len(step_ms)
+    if world > 1:
+        t = torch.tensor([ms_step], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = world * g.edges / (ms_step * 1e-3) / 1e9
+
+    # one extra solve counting the guarded atomics for the byte model
+    st_atom = ctx.run_device(g.nodes, g.edges, d_ni.data_ptr(), d_nl.data_ptr(), d_ew.data_ptr(),
+                             d_out.data_ptr(), opts=E.make_opts(mode=mode, quantile=args.quantile,
+                                                                degree_split=args.split, flags=E.FLAG_STATS),
+                             stream=stream.cuda_stream, stats=True)
+    inmst = d_out[: g.edges].cpu().numpy()
+    fw = int(g.eweight[inmst.astype(bool)].astype(np.int64).sum()) % 2**64
+
+    # end to end through the C ABI with host buffers (pinned), H2D + solve + D2H per step
+    h_ni = torch.from_numpy(g.nindex).pin_memory().numpy()
+    h_nl = torch.from_numpy(g.nlist).pin_memory().numpy()
+    h_ew = torch.from_numpy(g.eweight).pin_memory().numpy()
+    h_out = torch.empty(max(g.edges, 1), dtype=torch.uint8).pin_memory().numpy()
+    hg = E.Graph(h_ni, h_nl, h_ew)
+    hg.nindex, hg.nlist, hg.eweight = h_ni, h_nl, h_ew
+    for _ in range(2):
+        ctx.run_host(hg, opts, out=h_out, stats=False)
+    e2e_s = []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        ctx.run_host(hg, opts, out=h_out, stats=False)
+        e2e_s.append(time.perf_counter() - t1)
+    e2e_mean = sum(e2e_s) / len(e2e_s)
+    if world > 1:
+        t = torch.tensor([e2e_mean], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_mean = float(t.item())
+    h2d = 4 * (g.nodes + 1) + 8 * g.edges
+    d2h = g.edges
+
+    peak, peak_kind = load_peaks()
+    rb = round_kernel_bytes(last, atomics=st_atom["atomics"])
+    sb = scan_kernel_bytes(last, g.nodes, g.edges)
+    r_ms = sum(round_ms) / len(round_ms)
+    s_ms = sum(scan_ms) / len(scan_ms)
+    kernels = {
+        "rounds": {"bytes": rb, "ms": r_ms, "gbs": rb / (r_ms * 1e-3) / 1e9},
+        "scan": {"bytes": sb, "ms": s_ms, "gbs": sb / (s_ms * 1e-3) / 1e9},
+    }
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(args.workload, {}).get(dom)
+    roofline = {"bound": "hbm", "kernel": "k_rounds (both phases)" if dom == "rounds" else "k_scan (light+heavy)",
+                "achieved": kernels[dom]["gbs"], "peak": peak, "unit": "GB/s",
+                "frac": kernels[dom]["gbs"] / peak, "peak_source": peak_kind, "traffic": traffic,
+                "per_kernel": kernels}
+
+    # the plain form: the reference ECL_MST.cu rebuilt for sm_100a, same graph, same GPU
+    plain = None
+    plain_so = os.path.join(ROOT, "baseline", "_ref", "libecl_plain.so")
+    if rank == 0 and not args.no_plain and os.path.exists(plain_so) and world == 1:
+        import ctypes
+        lib = ctypes.CDLL(plain_so)
+        P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        f, th = ctypes.c_int(), ctypes.c_int()
+        lib.plain_threshold(g.nodes, g.edges, P(g.eweight), ctypes.byref(f), ctypes.byref(th))
+        pout = np.zeros(max(g.edges, 1), np.uint8)
+        secs = []
+        for i in range(5):
+            s = ctypes.c_double()
+            lib.plain_gpu_mst(g.nodes, g.edges, P(g.nindex), P(g.nlist), P(g.eweight), f, th, P(pout),
+                              ctypes.byref(s))
+            secs.append(s.value)
+        med = statistics.median(secs[1:])
+        plain = {"value": g.edges / med / 1e9, "unit": "Gedges/s", "ms": med * 1e3,
+                 "runs": len(secs) - 1, "inMST_identical": bool(np.array_equal(pout[: g.edges], inmst)),
+                 "what": "reference ECL_MST.cu gpuMST rebuilt for sm_100a, its own timed window, median"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib as O
+        if O.have_ref():
+            t1 = time.perf_counter()
+            ref_out = O.ref_cpu_mst(g.nindex, g.nlist, g.eweight)
+            dt = time.perf_counter() - t1
+            cpu = {"value": g.edges / dt / 1e9, "unit": "Gedges/s", "cores": 1, "kind": "reference",
+                   "sample": f"reference cpuMST (serial Kruskal) on the full workload, {dt:.1f} s, "
+                             f"host has {os.cpu_count()} cores",
+                   "inMST_identical": bool(np.array_equal(ref_out, inmst))}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gedges/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32/uint64", "data": "synthetic",
+            "config": {"workload": args.workload, "graph": desc, "nodes": g.nodes, "edges": g.edges,
+                       "threshold_mode": args.mode, "threshold": last["threshold"],
+                       "filtered": last["filtered"], "degree_split": last["degree_split"],
+                       "rounds": last["rounds"], "l2": "flushed between steps (256 MB write)",
+                       "parallelism": "replicas only" if world > 1 else "1 GPU",
+                       "ms_median": statistics.median(step_ms), "gen_s": round(gen_s, 2)},
+            "e2e": {"value": world * g.edges / e2e_mean / 1e9, "unit": "Gedges/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms": e2e_mean * 1e3},
+            "gpu_launches": 5 * args.steps,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "plain_ecl_mst": plain,
+            "vs_plain": (value / plain["value"]) if plain else None,
+            "forest_weight": fw,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,224 @@
+/*
+ * ecl_mst.h -- C ABI of the B200 (sm_100a) ECL-MST minimum spanning forest.
+ *
+ * The ABI replaces one in-file interface of the reference artifact
+ * (alexfallin/MST-Artifact-SC23):
+ *
+ *   ECL-MST/ECLgraph.h:29-35     struct ECLgraph {int nodes, edges; int *nindex, *nlist, *eweight;}
+ *   ECL-MST/ECLgraph.h:37-64     ECLgraph readECLgraph(const char*)
+ *   ECL-MST/ECLgraph.h:66-80     void writeECLgraph(const ECLgraph, const char*)
+ *   ECL-MST/ECLgraph.h:82-90     void freeECLgraph(ECLgraph&)
+ *   ECL-MST/ECL_MST.cu:265-362   template<bool filter> bool* gpuMST(const ECLgraph&, int threshold)
+ *   ECL-MST/ECL_MST.cu:389-395,
+ *                      :432-444  threshold heuristic (20 hashed samples, "300% of nodes")
+ *   ECL-MST/ECL_MST.cu:410-419   weight synthesis for weightless inputs
+ *   ECL-MST/ECL_MST.cu:365-386   verify()
+ *
+ * Differences in behaviour, all deliberate:
+ *   - nothing here calls exit(); every entry point returns an ecl_status code;
+ *   - the caller owns every buffer (inMST is caller-allocated, m bytes);
+ *   - malformed CSR content (nindex not monotone, neighbour ids out of range) is
+ *     reported as ECL_ERR_FORMAT instead of reading out of bounds.
+ *
+ * Output contract (identical to the reference GPU path): inMST[j] == 1 iff the
+ * CSR entry j = (v -> nlist[j]) with nlist[j] > v is an edge of the minimum
+ * spanning forest under the strict order (uint32(eweight[j]), j); all other
+ * entries, including the reverse direction of every forest edge, are 0.
+ */
+#ifndef ECL_MST_B200_H
+#define ECL_MST_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum ecl_status {
+  ECL_OK = 0,
+  ECL_ERR_INVALID_ARG = -1, /* NULL pointer, nodes < 1, edges < 0, bad option   */
+  ECL_ERR_IO = -2,          /* file could not be opened / read / written        */
+  ECL_ERR_FORMAT = -3,      /* truncated file or inconsistent CSR content        */
+  ECL_ERR_ALLOC = -4,       /* host or device allocation failed                 */
+  ECL_ERR_CUDA = -5,        /* a CUDA runtime call failed                        */
+  ECL_ERR_NO_DEVICE = -6,   /* no CUDA device is visible                         */
+  ECL_ERR_OVERFLOW = -7,    /* a worklist or batch exceeded its capacity        */
+  ECL_ERR_TIMEOUT = -8,     /* a device-side wait hit its limit (no hang)        */
+  ECL_ERR_TOO_LARGE = -9,   /* input beyond a stated maximum                     */
+  ECL_ERR_UNSUPPORTED = -10 /* option not available in this build / device      */
+} ecl_status;
+
+/* Human-readable name of a status code (static string). */
+const char* ecl_status_string(int status);
+
+/* ------------------------------------------------------------------ graph */
+/* Byte-for-byte the reference ECLgraph (ECLgraph.h:29-35). The arrays are
+ * host pointers for the host entry points and device pointers for the
+ * *_device entry points. eweight may be NULL (weightless file). */
+typedef struct ecl_graph {
+  int32_t nodes;
+  int32_t edges;
+  int32_t* nindex; /* nodes + 1 */
+  int32_t* nlist;  /* edges     */
+  int32_t* eweight;/* edges, or NULL */
+} ecl_graph;
+
+/* Read a binary ECLgraph file (replaces readECLgraph, ECLgraph.h:37-64).
+ * Layout: int32 nodes, int32 edges, int32 nindex[nodes+1], int32 nlist[edges],
+ * optionally int32 eweight[edges]. A file that ends right after nlist yields
+ * eweight == NULL, as in the reference. Arrays are malloc'd; free them with
+ * ecl_free_graph. */
+int ecl_read_graph(const char* path, ecl_graph* out);
+
+/* Write a binary ECLgraph file (replaces writeECLgraph, ECLgraph.h:66-80). */
+int ecl_write_graph(const ecl_graph* g, const char* path);
+
+/* Free arrays allocated by ecl_read_graph / ecl_gen_* (replaces freeECLgraph,
+ * ECLgraph.h:82-90). Sets the pointers to NULL. */
+void ecl_free_graph(ecl_graph* g);
+
+/* Weights for a weightless graph, bit-exact with ECL_MST.cu:410-419:
+ * eweight[j] = |1 + (int32 wrap(v * nlist[j]) % nodes)| for j in row v.
+ * g->eweight must point to a caller-allocated array of g->edges ints. */
+int ecl_synthesize_weights(ecl_graph* g);
+
+/* Check CSR consistency on the host: nindex[0] == 0, nindex monotone,
+ * nindex[nodes] == edges, 0 <= nlist[j] < nodes. Returns ECL_OK or
+ * ECL_ERR_FORMAT. */
+int ecl_validate_graph(const ecl_graph* g);
+
+/* ---------------------------------------------------------- synthetic inputs */
+/* Seeded, deterministic generators. Every graph is deduplicated, free of
+ * self-loops, symmetric, with rows sorted by neighbour id, and each undirected
+ * edge {u,v} carries one weight drawn uniformly from [1, wmax] from a hash of
+ * (seed, min(u,v), max(u,v)) and mirrored to both directions. Arrays are
+ * malloc'd (free with ecl_free_graph). threads <= 0 means all host cores. */
+int ecl_gen_grid(int32_t rows, int32_t cols, uint64_t seed, int32_t wmax,
+                 int threads, ecl_graph* out);
+int ecl_gen_er(int32_t nodes, double avg_degree, uint64_t seed, int32_t wmax,
+               int threads, ecl_graph* out);
+int ecl_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b,
+                 double c, uint64_t seed, int32_t wmax, int threads,
+                 ecl_graph* out);
+int ecl_gen_rgg2d(int32_t nodes, double avg_degree, uint64_t seed,
+                  int32_t wmax, int threads, ecl_graph* out);
+
+/* ------------------------------------------------------------- threshold */
+typedef enum ecl_threshold_mode {
+  ECL_THRESH_HEURISTIC = 0, /* the reference rule (ECL_MST.cu:408,432-444)      */
+  ECL_THRESH_NONE = 1,      /* single unfiltered phase (gpuMST<false>, INT_MAX) */
+  ECL_THRESH_EXPLICIT = 2,  /* opts.threshold                                   */
+  ECL_THRESH_QUANTILE = 3,  /* opts.quantile of a 4096-entry weight sample      */
+  ECL_THRESH_LEARNED = 4    /* quantile + split predicted by the trained MLP     */
+} ecl_threshold_mode;
+
+/* The reference threshold heuristic on host arrays. *filtered = 1 iff
+ * edges/nodes >= 4 (integer division); the threshold is then the
+ * min(19, int(3.0*nodes*20/edges))-th smallest of 20 weights sampled at
+ * hash(i) % edges. *filtered = 0 gives threshold INT32_MAX. */
+int ecl_heuristic_threshold(const ecl_graph* g, int32_t* threshold,
+                            int32_t* filtered);
+
+/* --------------------------------------------------------------- options */
+enum {
+  ECL_FLAG_L2_PERSIST = 1 << 0, /* L2 access-policy window on parent/min slots   */
+  ECL_FLAG_STATS = 1 << 1,      /* count guarded atomics (slower; off in timing) */
+  ECL_FLAG_NO_SMALL_TAIL = 1 << 2 /* keep every round grid-wide (ablation)      */
+};
+
+typedef struct mst_opts {
+  int32_t threshold_mode; /* ecl_threshold_mode                              */
+  int32_t threshold;      /* ECL_THRESH_EXPLICIT: edges with w <= threshold    */
+                          /* form the first (light) phase                      */
+  float quantile;         /* ECL_THRESH_QUANTILE, in [0,1]; >= 1 disables      */
+  int32_t degree_split;   /* rows with degree >= split are scanned by warps in */
+                          /* 128-entry chunks, shorter rows by one thread;     */
+                          /* 0 = default (32)                                  */
+  int32_t block_size;     /* threads per CTA of the round kernel, 0 = default  */
+  int32_t ctas_per_sm;    /* 0 = as many as fit                                */
+  int32_t small_tail;     /* worklist size at which one CTA finishes the      */
+                          /* rounds alone; 0 = default, < 0 = never            */
+  int32_t flags;          /* ECL_FLAG_*                                        */
+  int32_t reserved[8];
+} mst_opts;
+
+/* Fill *opts with the defaults (heuristic threshold, reference semantics). */
+void ecl_default_opts(mst_opts* opts);
+
+/* Per-run counters, filled when a stats pointer is passed. */
+#define ECL_MAX_ROUNDS 64
+typedef struct ecl_mst_stats {
+  int32_t threshold;       /* threshold used (INT32_MAX when unfiltered)        */
+  int32_t filtered;        /* 1 if two phases ran                               */
+  int32_t degree_split;    /* split used by the scans                           */
+  int32_t rounds[2];       /* Boruvka rounds of the light / heavy phase         */
+  int32_t status;          /* device error word (0 = clean)                     */
+  int64_t scan_kept[2];    /* worklist entries appended by each scan            */
+  int64_t wl_in[2][ECL_MAX_ROUNDS];  /* worklist size entering each round      */
+  int64_t atomics;         /* guarded atomicMin issued (ECL_FLAG_STATS only)    */
+  int64_t forest_edges;    /* number of inMST entries set                       */
+  uint64_t forest_weight;  /* sum of eweight over inMST (as verify(), :377)     */
+  float ms_total;          /* device time of the whole solve (CUDA events)      */
+  float ms_rounds;         /* device time of the round kernels                  */
+  float ms_scan;           /* device time of the scan kernels                   */
+} ecl_mst_stats;
+
+/* ------------------------------------------------------------- the solve */
+/* One-shot drop-in for gpuMST (ECL_MST.cu:265-362) plus the heuristic choice
+ * of main (:432-444): host CSR in, caller-allocated host inMST (edges bytes)
+ * out. Allocates and frees its own device workspace on the current device.
+ * opts == NULL means ecl_default_opts. stats may be NULL. */
+int ecl_mst_run(const ecl_graph* g, uint8_t* inMST, const mst_opts* opts,
+                ecl_mst_stats* stats);
+
+/* Reusable device workspace, sized for graphs up to (max_nodes, max_edges).
+ * Creating it allocates; runs through it allocate nothing. */
+typedef struct ecl_mst_ctx ecl_mst_ctx;
+int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edges,
+                       ecl_mst_ctx** out);
+void ecl_mst_ctx_destroy(ecl_mst_ctx* ctx);
+
+/* Host CSR in, host inMST out, through the context's device buffers and the
+ * context's stream: H2D copies, the solve and the D2H copy of inMST. */
+int ecl_mst_ctx_run_host(ecl_mst_ctx* ctx, const ecl_graph* g, uint8_t* inMST,
+                         const mst_opts* opts, ecl_mst_stats* stats);
+
+/* Device-resident solve: d_graph holds DEVICE pointers, d_inMST is a device
+ * buffer of edges bytes. Enqueued on `stream` (cudaStream_t, NULL = the
+ * context's stream); returns after enqueueing unless stats != NULL, in which
+ * case it synchronises and fills stats. Errors found on the device are
+ * returned by ecl_mst_ctx_sync. */
+int ecl_mst_run_device(ecl_mst_ctx* ctx, const ecl_graph* d_graph,
+                       uint8_t* d_inMST, const mst_opts* opts, void* stream,
+                       ecl_mst_stats* stats);
+
+/* Wait for the context's stream and report a device-side error if any. */
+int ecl_mst_ctx_sync(ecl_mst_ctx* ctx);
+
+/* The stream the context enqueues on (a cudaStream_t). */
+void* ecl_mst_ctx_stream(ecl_mst_ctx* ctx);
+
+/* Pinned host memory for fast H2D/D2H (cudaHostAlloc / cudaFreeHost). */
+int ecl_host_alloc_pinned(size_t bytes, void** out);
+void ecl_host_free_pinned(void* p);
+
+/* ---------------------------------------------------------------- verify */
+/* Restates verify() (ECL_MST.cu:365-386): per-entry comparison of two inMST
+ * arrays and their uint64 forest weights. Returns 1 if they agree (no entry in
+ * only one of them and equal weights), 0 otherwise; counts may be NULL
+ * (4 int64: both, neither, only_a, only_b). */
+int ecl_verify(const ecl_graph* g, const uint8_t* a, const uint8_t* b,
+               int64_t counts[4], uint64_t* weight_a, uint64_t* weight_b);
+
+/* uint64 sum of eweight over set inMST entries (as verify(), :377-378). */
+uint64_t ecl_forest_weight(const ecl_graph* g, const uint8_t* inMST);
+
+/* Library version string. */
+const char* ecl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ECL_MST_B200_H */

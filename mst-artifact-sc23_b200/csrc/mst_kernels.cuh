@@ -1,0 +1,191 @@
+// Device building blocks of the B200 ECL-MST engine: coherent loads, the
+// bounded grid barrier, CTA-aggregated worklist reservation, find with path
+// halving and the CAS union. Shared by the single-graph engine (ecl_mst.cu)
+// and the batched engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ecl_mst.h"
+
+namespace ecl {
+
+typedef unsigned long long u64;
+
+// Device error word bits (DevState::error).
+enum : unsigned {
+  kErrFormat = 1u,    // nindex not monotone / out of range, or nlist id >= nodes
+  kErrOverflow = 2u,  // a worklist or descriptor buffer ran out of room
+  kErrTimeout = 4u,   // a grid barrier waited past its limit
+  kErrRounds = 8u     // more Boruvka rounds than ECL_MAX_ROUNDS
+};
+
+constexpr int kChunkLog = 7;  // long rows are scanned in aligned 128-entry chunks
+constexpr int kChunk = 1 << kChunkLog;
+constexpr u64 kNoEdge = ~0ull;
+
+// Control block of one solve, zeroed before every solve.
+struct DevState {
+  int threshold;       // light phase keeps w <= threshold
+  int filtered;        // 1 = light + heavy phase, 0 = one unfiltered phase
+  int split;           // degree split between the thread and the chunk tier
+  unsigned error;      // kErr* bits
+  unsigned bar_count;  // grid barrier: CTAs arrived in the current generation
+  unsigned bar_gen;    // grid barrier: generation counter
+  int rounds[2];       // Boruvka rounds per phase
+  unsigned desc_count; // long-row chunk descriptors emitted by the current scan
+  unsigned pad;
+  float quantile;      // learned / quantile modes: filter quantile in [0,1]
+  int learned_split;   // learned mode: predicted degree split
+  u64 atomics;         // guarded atomicMin issued (stats mode)
+  unsigned wl_count[2][ECL_MAX_ROUNDS + 1];  // [phase][r] = entries entering round r
+};
+
+__device__ __forceinline__ u64 globaltimer_ns() {
+  u64 t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned ld_volatile(const unsigned* p) {
+  return *(const volatile unsigned*)p;
+}
+
+// Grid-wide barrier for cooperative launches. Every wait is bounded by
+// `timeout_ns`; on expiry the kErrTimeout bit is set and all later barriers
+// return at once, so a stuck CTA turns into an error status instead of a hang.
+// Returns false once the timeout bit is set.
+__device__ __forceinline__ bool grid_barrier(DevState* st, u64 timeout_ns) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned gen = ld_volatile(&st->bar_gen);
+    __threadfence();
+    const unsigned arrived = atomicAdd(&st->bar_count, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(&st->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&st->bar_gen, 1u);
+    } else {
+      const u64 t0 = globaltimer_ns();
+      unsigned ns = 32;
+      while (ld_volatile(&st->bar_gen) == gen) {
+        if (ld_volatile(&st->error) & kErrTimeout) break;
+        if (globaltimer_ns() - t0 > timeout_ns) {
+          atomicOr(&st->error, kErrTimeout);
+          break;
+        }
+        __nanosleep(ns);
+        if (ns < 256) ns <<= 1;
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return (ld_volatile(&st->error) & kErrTimeout) == 0;
+}
+
+// Shared memory of one CTA-wide two-counter reservation.
+struct ReserveSmem {
+  unsigned warp_off[32][2];
+  unsigned base[2];
+};
+
+// CTA-aggregated reservation of c0 slots in counter ctr0 and c1 slots in
+// counter ctr1 (ctr1 may be null when every c1 is 0): one warp-shuffle scan,
+// one scan over warp totals and at most one global atomic per counter per CTA.
+// Every thread of the CTA must call it (it contains __syncthreads).
+__device__ __forceinline__ void cta_reserve2(unsigned c0, unsigned c1, unsigned* ctr0,
+                                             unsigned* ctr1, ReserveSmem& sm, unsigned& pos0,
+                                             unsigned& pos1) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned s0 = c0, s1 = c1;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t0 = __shfl_up_sync(0xffffffffu, s0, o);
+    const unsigned t1 = __shfl_up_sync(0xffffffffu, s1, o);
+    if (lane >= o) {
+      s0 += t0;
+      s1 += t1;
+    }
+  }
+  if (lane == 31) {
+    sm.warp_off[warp][0] = s0;
+    sm.warp_off[warp][1] = s1;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    const unsigned w0 = lane < nw ? sm.warp_off[lane][0] : 0u;
+    const unsigned w1 = lane < nw ? sm.warp_off[lane][1] : 0u;
+    unsigned x0 = w0, x1 = w1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t0 = __shfl_up_sync(0xffffffffu, x0, o);
+      const unsigned t1 = __shfl_up_sync(0xffffffffu, x1, o);
+      if (lane >= o) {
+        x0 += t0;
+        x1 += t1;
+      }
+    }
+    if (lane < nw) {
+      sm.warp_off[lane][0] = x0 - w0;
+      sm.warp_off[lane][1] = x1 - w1;
+    }
+    if (lane == 31) {
+      sm.base[0] = x0 ? atomicAdd(ctr0, x0) : 0u;
+      sm.base[1] = x1 ? atomicAdd(ctr1, x1) : 0u;
+    }
+  }
+  __syncthreads();
+  pos0 = sm.base[0] + sm.warp_off[warp][0] + (s0 - c0);
+  pos1 = sm.base[1] + sm.warp_off[warp][1] + (s1 - c1);
+  __syncthreads();
+}
+
+// Root of v. parent[] only ever points to smaller or equal ids, so the walk
+// ends. Path splitting (each visited node is re-pointed to its grandparent)
+// is applied on the way: it only shortcuts inside one tree, so concurrent
+// finds still reach the same root, and it bounds the cost of long hook chains
+// (a path graph with increasing weights hooks every vertex under its
+// predecessor in one round). Must not run concurrently with unions.
+__device__ __forceinline__ int find_halve(int v, int* parent) {
+  int p = __ldcg(parent + v);
+  while (p != v) {
+    const int gp = __ldcg(parent + p);
+    if (gp != p) __stcg(parent + v, gp);
+    v = p;
+    p = gp;
+  }
+  return v;
+}
+
+// Read-only root walk (no writes); safe next to unions.
+__device__ __forceinline__ int find_ro(int v, const int* parent) {
+  int p = __ldcg(parent + v);
+  while (p != v) {
+    v = p;
+    p = __ldcg(parent + v);
+  }
+  return v;
+}
+
+// Union of the trees holding a and b by CAS-hooking the larger root under the
+// smaller id. A failed CAS returns the node's current parent, which is smaller,
+// so the larger id of the pair strictly decreases and the loop ends.
+__device__ __forceinline__ void cas_union(int a, int b, int* parent) {
+  while (true) {
+    const int hi = a > b ? a : b, lo = a > b ? b : a;
+    if (hi == lo) return;
+    const int old = atomicCAS(parent + hi, hi, lo);
+    if (old == hi) return;
+    a = lo;
+    b = old;
+  }
+}
+
+// Tuple key of an edge: (uint32 weight, edge index), as ((ull)w << 32) | j.
+__device__ __forceinline__ u64 edge_key(int w, int j) {
+  return ((u64)(unsigned)w << 32) | (u64)(unsigned)j;
+}
+
+}  // namespace ecl

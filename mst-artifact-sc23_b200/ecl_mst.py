@@ -1,0 +1,296 @@
+"""Python binding of the ecl_mst C ABI (include/ecl_mst.h) via ctypes.
+
+It mirrors the reference's interface for this path (alexfallin/MST-Artifact-SC23):
+  - ``Graph``: the ECLgraph struct (ECL-MST/ECLgraph.h:29-35) as numpy arrays;
+  - ``read_graph`` / ``write_graph``: readECLgraph / writeECLgraph (ECLgraph.h:37-80);
+  - ``mst``: gpuMST<filter> plus main's threshold choice (ECL_MST.cu:265-362, :432-444),
+    returning the per-CSR-entry ``inMST`` flags (uint8, edges long);
+  - ``verify``: verify() (ECL_MST.cu:365-386).
+
+There is no fallback: if ``libecl_mst.so`` (built by ``make`` in this directory)
+is missing, ``load()`` raises. Errors from the library come back as
+``EclError`` with the library's status code (the reference would exit(-1)).
+"""
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_uint64, c_void_p
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libecl_mst.so")
+
+ECL_OK = 0
+STATUS = {
+    0: "ok", -1: "invalid argument", -2: "i/o error", -3: "malformed graph",
+    -4: "allocation failed", -5: "CUDA error", -6: "no CUDA device",
+    -7: "capacity exceeded", -8: "device wait limit reached",
+    -9: "input exceeds the supported maximum", -10: "unsupported option",
+}
+THRESH_HEURISTIC, THRESH_NONE, THRESH_EXPLICIT, THRESH_QUANTILE, THRESH_LEARNED = range(5)
+FLAG_L2_PERSIST, FLAG_STATS, FLAG_NO_SMALL_TAIL = 1, 2, 4
+MAX_ROUNDS = 64
+
+
+class EclError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS.get(status, 'unknown')} ({status})")
+
+
+class EclGraphC(ctypes.Structure):
+    _fields_ = [("nodes", c_int32), ("edges", c_int32), ("nindex", c_void_p),
+                ("nlist", c_void_p), ("eweight", c_void_p)]
+
+
+class MstOpts(ctypes.Structure):
+    _fields_ = [("threshold_mode", c_int32), ("threshold", c_int32), ("quantile", c_float),
+                ("degree_split", c_int32), ("block_size", c_int32), ("ctas_per_sm", c_int32),
+                ("small_tail", c_int32), ("flags", c_int32), ("reserved", c_int32 * 8)]
+
+
+class MstStats(ctypes.Structure):
+    _fields_ = [("threshold", c_int32), ("filtered", c_int32), ("degree_split", c_int32),
+                ("rounds", c_int32 * 2), ("status", c_int32), ("scan_kept", c_int64 * 2),
+                ("wl_in", (c_int64 * MAX_ROUNDS) * 2), ("atomics", c_int64),
+                ("forest_edges", c_int64), ("forest_weight", c_uint64),
+                ("ms_total", c_float), ("ms_rounds", c_float), ("ms_scan", c_float)]
+
+    def as_dict(self):
+        return {
+            "threshold": self.threshold, "filtered": self.filtered,
+            "degree_split": self.degree_split, "rounds": list(self.rounds),
+            "status": self.status, "scan_kept": list(self.scan_kept),
+            "wl_in": [[int(x) for x in self.wl_in[p][: max(self.rounds[p], 0) + 1]] for p in range(2)],
+            "atomics": self.atomics, "forest_edges": self.forest_edges,
+            "forest_weight": self.forest_weight, "ms_total": self.ms_total,
+            "ms_rounds": self.ms_rounds, "ms_scan": self.ms_scan,
+        }
+
+
+_lib = None
+
+
+def load():
+    """Load libecl_mst.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run `make` in {_HERE} (no CPU fallback exists)")
+    lib = ctypes.CDLL(LIB_PATH)
+    G = POINTER(EclGraphC)
+    sig = {
+        "ecl_status_string": (c_char_p, [c_int]),
+        "ecl_version": (c_char_p, []),
+        "ecl_read_graph": (c_int, [c_char_p, G]),
+        "ecl_write_graph": (c_int, [G, c_char_p]),
+        "ecl_free_graph": (None, [G]),
+        "ecl_synthesize_weights": (c_int, [G]),
+        "ecl_validate_graph": (c_int, [G]),
+        "ecl_gen_grid": (c_int, [c_int32, c_int32, c_uint64, c_int32, c_int, G]),
+        "ecl_gen_er": (c_int, [c_int32, c_double, c_uint64, c_int32, c_int, G]),
+        "ecl_gen_rmat": (c_int, [c_int32, c_int32, c_double, c_double, c_double, c_uint64, c_int32, c_int, G]),
+        "ecl_gen_rgg2d": (c_int, [c_int32, c_double, c_uint64, c_int32, c_int, G]),
+        "ecl_heuristic_threshold": (c_int, [G, POINTER(c_int32), POINTER(c_int32)]),
+        "ecl_default_opts": (None, [POINTER(MstOpts)]),
+        "ecl_mst_run": (c_int, [G, c_void_p, POINTER(MstOpts), POINTER(MstStats)]),
+        "ecl_mst_ctx_create": (c_int, [c_int, c_int64, c_int64, POINTER(c_void_p)]),
+        "ecl_mst_ctx_destroy": (None, [c_void_p]),
+        "ecl_mst_ctx_run_host": (c_int, [c_void_p, G, c_void_p, POINTER(MstOpts), POINTER(MstStats)]),
+        "ecl_mst_run_device": (c_int, [c_void_p, G, c_void_p, POINTER(MstOpts), c_void_p, POINTER(MstStats)]),
+        "ecl_mst_ctx_sync": (c_int, [c_void_p]),
+        "ecl_mst_ctx_stream": (c_void_p, [c_void_p]),
+        "ecl_host_alloc_pinned": (c_int, [ctypes.c_size_t, POINTER(c_void_p)]),
+        "ecl_host_free_pinned": (None, [c_void_p]),
+        "ecl_verify": (c_int, [G, c_void_p, c_void_p, POINTER(c_int64), POINTER(c_uint64), POINTER(c_uint64)]),
+        "ecl_forest_weight": (c_uint64, [G, c_void_p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(status, what):
+    if status != ECL_OK:
+        raise EclError(status, what)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(c_void_p)
+
+
+class Graph:
+    """ECLgraph: int32 CSR (nindex[nodes+1], nlist[edges], optional eweight[edges])."""
+
+    def __init__(self, nindex, nlist, eweight=None):
+        self.nindex = np.ascontiguousarray(nindex, dtype=np.int32)
+        self.nlist = np.ascontiguousarray(nlist, dtype=np.int32)
+        self.eweight = None if eweight is None else np.ascontiguousarray(eweight, dtype=np.int32)
+        self.nodes = int(self.nindex.shape[0]) - 1
+        self.edges = int(self.nlist.shape[0])
+
+    def struct(self):
+        return EclGraphC(self.nodes, self.edges, _ptr(self.nindex), _ptr(self.nlist), _ptr(self.eweight))
+
+    @classmethod
+    def _from_c(cls, gc):
+        lib = load()
+        n, m = gc.nodes, gc.edges
+        nindex = np.ctypeslib.as_array(ctypes.cast(gc.nindex, POINTER(c_int32)), (n + 1,)).copy()
+        if m > 0:
+            nlist = np.ctypeslib.as_array(ctypes.cast(gc.nlist, POINTER(c_int32)), (m,)).copy()
+            ew = (np.ctypeslib.as_array(ctypes.cast(gc.eweight, POINTER(c_int32)), (m,)).copy()
+                  if gc.eweight else None)
+        else:
+            nlist = np.zeros(0, np.int32)
+            ew = np.zeros(0, np.int32) if gc.eweight else None
+        lib.ecl_free_graph(ctypes.byref(gc))
+        return cls(nindex, nlist, ew)
+
+
+def read_graph(path):
+    gc = EclGraphC()
+    _check(load().ecl_read_graph(os.fsencode(path), ctypes.byref(gc)), f"read {path}")
+    return Graph._from_c(gc)
+
+
+def write_graph(g, path):
+    gs = g.struct()
+    _check(load().ecl_write_graph(ctypes.byref(gs), os.fsencode(path)), f"write {path}")
+
+
+def synthesize_weights(g):
+    """Fill g.eweight with the reference's synthetic weights (ECL_MST.cu:410-419)."""
+    g.eweight = np.zeros(g.edges, np.int32)
+    gs = g.struct()
+    _check(load().ecl_synthesize_weights(ctypes.byref(gs)), "synthesize_weights")
+    return g
+
+
+def validate_graph(g):
+    gs = g.struct()
+    return load().ecl_validate_graph(ctypes.byref(gs))
+
+
+def gen_grid(rows, cols, seed, wmax, threads=0):
+    gc = EclGraphC()
+    _check(load().ecl_gen_grid(rows, cols, seed, wmax, threads, ctypes.byref(gc)), "gen_grid")
+    return Graph._from_c(gc)
+
+
+def gen_er(nodes, avg_degree, seed, wmax, threads=0):
+    gc = EclGraphC()
+    _check(load().ecl_gen_er(nodes, avg_degree, seed, wmax, threads, ctypes.byref(gc)), "gen_er")
+    return Graph._from_c(gc)
+
+
+def gen_rmat(scale, edge_factor, a, b, c, seed, wmax, threads=0):
+    gc = EclGraphC()
+    _check(load().ecl_gen_rmat(scale, edge_factor, a, b, c, seed, wmax, threads, ctypes.byref(gc)), "gen_rmat")
+    return Graph._from_c(gc)
+
+
+def gen_rgg2d(nodes, avg_degree, seed, wmax, threads=0):
+    gc = EclGraphC()
+    _check(load().ecl_gen_rgg2d(nodes, avg_degree, seed, wmax, threads, ctypes.byref(gc)), "gen_rgg2d")
+    return Graph._from_c(gc)
+
+
+def heuristic_threshold(g):
+    """(threshold, filtered) of the reference rule (ECL_MST.cu:408,432-440)."""
+    t, f = c_int32(), c_int32()
+    gs = g.struct()
+    _check(load().ecl_heuristic_threshold(ctypes.byref(gs), ctypes.byref(t), ctypes.byref(f)), "heuristic")
+    return t.value, f.value
+
+
+def make_opts(mode=THRESH_HEURISTIC, threshold=0, quantile=1.0, degree_split=0, small_tail=0, flags=0):
+    o = MstOpts()
+    load().ecl_default_opts(ctypes.byref(o))
+    o.threshold_mode = mode
+    o.threshold = threshold
+    o.quantile = quantile
+    o.degree_split = degree_split
+    o.small_tail = small_tail
+    o.flags = flags
+    return o
+
+
+def mst(g, opts=None):
+    """One-shot solve (ecl_mst_run): returns (inMST uint8[edges], stats dict)."""
+    out = np.zeros(max(g.edges, 1), np.uint8)
+    st = MstStats()
+    gs = g.struct()
+    _check(load().ecl_mst_run(ctypes.byref(gs), _ptr(out), None if opts is None else ctypes.byref(opts),
+                              ctypes.byref(st)), "ecl_mst_run")
+    return out[: g.edges], st.as_dict()
+
+
+def verify(g, a, b):
+    """verify() of the reference: (agree, counts[4], weight_a, weight_b)."""
+    counts = (c_int64 * 4)()
+    wa, wb = c_uint64(), c_uint64()
+    gs = g.struct()
+    a = np.ascontiguousarray(a, np.uint8)
+    b = np.ascontiguousarray(b, np.uint8)
+    ok = load().ecl_verify(ctypes.byref(gs), _ptr(a), _ptr(b), counts, ctypes.byref(wa), ctypes.byref(wb))
+    return bool(ok), list(counts), wa.value, wb.value
+
+
+class Context:
+    """Reusable device workspace (ecl_mst_ctx)."""
+
+    def __init__(self, max_nodes, max_edges, device=0):
+        self._lib = load()
+        h = c_void_p()
+        _check(self._lib.ecl_mst_ctx_create(device, max_nodes, max_edges, ctypes.byref(h)), "ctx_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            self._lib.ecl_mst_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        return self._lib.ecl_mst_ctx_stream(self.handle)
+
+    def run_host(self, g, opts=None, out=None, stats=True):
+        """Host CSR in, host inMST out (H2D + solve + D2H)."""
+        if out is None:
+            out = np.zeros(max(g.edges, 1), np.uint8)
+        st = MstStats() if stats else None
+        gs = g.struct()
+        _check(self._lib.ecl_mst_ctx_run_host(self.handle, ctypes.byref(gs), _ptr(out),
+                                              None if opts is None else ctypes.byref(opts),
+                                              None if st is None else ctypes.byref(st)), "ctx_run_host")
+        return out[: g.edges], (st.as_dict() if st is not None else None)
+
+    def run_device(self, nodes, edges, d_nindex, d_nlist, d_eweight, d_inMST, opts=None, stream=None,
+                   stats=False):
+        """Device pointers in and out (ints). Enqueues; returns stats only if asked."""
+        gs = EclGraphC(nodes, edges, d_nindex, d_nlist, d_eweight)
+        st = MstStats() if stats else None
+        _check(self._lib.ecl_mst_run_device(self.handle, ctypes.byref(gs), d_inMST,
+                                            None if opts is None else ctypes.byref(opts), stream,
+                                            None if st is None else ctypes.byref(st)), "run_device")
+        return st.as_dict() if st is not None else None
+
+    def sync(self):
+        _check(self._lib.ecl_mst_ctx_sync(self.handle), "ctx_sync")

@@ -1,0 +1,199 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and with the
+reference itself rebuilt for sm_100a. Bit-exact inMST and equal uint64 forest
+weight on every input: integer work, so the tolerance is zero."""
+import numpy as np
+import pytest
+
+import ecl_mst as E
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+MODES = [
+    dict(),
+    dict(mode=E.THRESH_NONE),
+    dict(mode=E.THRESH_QUANTILE, quantile=0.05),
+    dict(mode=E.THRESH_QUANTILE, quantile=0.5),
+    dict(mode=E.THRESH_QUANTILE, quantile=0.95),
+    dict(degree_split=1),
+    dict(degree_split=4),
+    dict(degree_split=1 << 20),
+    dict(small_tail=-1),
+    dict(small_tail=1 << 30),
+    dict(mode=E.THRESH_QUANTILE, quantile=0.3, degree_split=2, small_tail=-1),
+]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = E.Context(1 << 22, 1 << 26)
+    yield c
+    c.close()
+
+
+def _graph(c):
+    return E.Graph(c["nindex"], c["nlist"], c["eweight"])
+
+
+def test_golden_one_shot_entry_point(golden):
+    for name, c in golden.items():
+        got, st = E.mst(_graph(c))
+        assert np.array_equal(got, c["inMST"]), name
+
+
+@pytest.mark.parametrize("kw", MODES, ids=[str(k) for k in MODES])
+def test_golden_every_schedule(ctx, golden, kw):
+    opts = E.make_opts(**kw)
+    for name, c in golden.items():
+        g = _graph(c)
+        got, st = ctx.run_host(g, opts)
+        assert st["status"] == 0, name
+        assert np.array_equal(got, c["inMST"]), (name, kw)
+        assert st["forest_weight"] == int(c["eweight"][c["inMST"].astype(bool)].astype(np.int64).sum()) % 2**64
+
+
+def test_golden_explicit_thresholds(ctx, golden):
+    rng = np.random.default_rng(3)
+    for name, c in golden.items():
+        if len(c["nlist"]) == 0:
+            continue
+        for t in list(rng.choice(c["eweight"], 3)) + [-1, 0, 2**31 - 1]:
+            got, _ = ctx.run_host(_graph(c), E.make_opts(mode=E.THRESH_EXPLICIT, threshold=int(t)))
+            assert np.array_equal(got, c["inMST"]), (name, t)
+
+
+def test_heuristic_threshold_on_device_matches_reference(ctx, golden):
+    for name, c in golden.items():
+        if len(c["nlist"]) == 0:
+            continue
+        _, st = ctx.run_host(_graph(c))
+        t, f = (int(x) for x in c["threshold"])
+        assert (st["threshold"], st["filtered"]) == (t, f), name
+
+
+def _families():
+    return [
+        ("grid_c1", lambda: E.gen_grid(1000, 1000, 1, 1_000_000)),
+        ("rmat16", lambda: E.gen_rmat(16, 16, 0.57, 0.19, 0.19, 2, 1 << 24)),
+        ("rmat18_ef8", lambda: E.gen_rmat(18, 8, 0.57, 0.19, 0.19, 21, 1 << 20)),
+        ("er", lambda: E.gen_er(200_000, 8, 5, 1 << 20)),
+        ("er_dense", lambda: E.gen_er(50_000, 32, 6, 1 << 30)),
+        ("rgg", lambda: E.gen_rgg2d(300_000, 3, 7, 1 << 20)),
+        ("grid_ties", lambda: E.gen_grid(300, 700, 3, 4)),
+    ]
+
+
+@pytest.mark.parametrize("name,make", _families(), ids=[f[0] for f in _families()])
+def test_generated_families_vs_oracle(ctx, name, make):
+    g = make()
+    t, f = E.heuristic_threshold(g)
+    want, w, fe = O.oracle_mst(g.nindex, g.nlist, g.eweight, t, f)
+    for kw in (dict(), dict(mode=E.THRESH_QUANTILE, quantile=0.1), dict(mode=E.THRESH_NONE),
+               dict(degree_split=8)):
+        got, st = ctx.run_host(g, E.make_opts(**kw))
+        assert st["status"] == 0
+        assert np.array_equal(got, want), (name, kw)
+        assert st["forest_weight"] == w and st["forest_edges"] == fe
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name,make", _families()[:4], ids=[f[0] for f in _families()[:4]])
+def test_vs_reference_rebuilt_for_sm100a(ctx, name, make):
+    g = make()
+    t, f = O.ref_threshold(g.nodes, g.eweight)
+    ref_out, _ = O.ref_gpu_mst(g.nindex, g.nlist, g.eweight, f, t)
+    got, _ = ctx.run_host(g)
+    assert np.array_equal(got, ref_out), name
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref not built")
+def test_negative_weights_follow_reference_gpu(ctx):
+    """With negative weights the reference GPU path orders weights as uint32
+    and splits phases by a signed compare; the default schedule reproduces it."""
+    rng = np.random.default_rng(7)
+    for s in range(4):
+        g = E.gen_er(3000, 10, 100 + s, 1000)
+        g.eweight = (g.eweight - 500).astype(np.int32)  # mirrored, some negative
+        t, f = O.ref_threshold(g.nodes, g.eweight)
+        ref_out, _ = O.ref_gpu_mst(g.nindex, g.nlist, g.eweight, f, t)
+        got, _ = ctx.run_host(g)
+        assert np.array_equal(got, ref_out)
+        ours, _, _ = O.oracle_mst(g.nindex, g.nlist, g.eweight, t, f)
+        assert np.array_equal(ours, ref_out)
+
+
+def test_device_entry_point_with_torch_buffers(ctx):
+    import torch
+    g = E.gen_rmat(15, 16, 0.57, 0.19, 0.19, 9, 1 << 24)
+    want, _, _ = O.oracle_mst(g.nindex, g.nlist, g.eweight, *E.heuristic_threshold(g))
+    dev = torch.device("cuda:0")
+    ni = torch.from_numpy(g.nindex).to(dev)
+    nl = torch.from_numpy(g.nlist).to(dev)
+    ew = torch.from_numpy(g.eweight).to(dev)
+    out = torch.empty(g.edges, dtype=torch.uint8, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        out.fill_(7)
+        ctx.run_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(),
+                       stream=s)
+        torch.cuda.synchronize()
+        ctx.sync()
+        assert np.array_equal(out.cpu().numpy(), want)
+
+
+def test_context_reuse_across_graphs(ctx, golden):
+    names = list(golden)
+    for name in names + names[::-1]:
+        c = golden[name]
+        got, _ = ctx.run_host(_graph(c))
+        assert np.array_equal(got, c["inMST"]), name
+
+
+def test_out_of_range_neighbour_is_reported_not_read(ctx):
+    g = E.gen_grid(50, 50, 1, 100)
+    nl = g.nlist.copy()
+    nl[17] = g.nodes + 5
+    with pytest.raises(E.EclError) as ei:
+        ctx.run_host(E.Graph(g.nindex, nl, g.eweight))
+    assert ei.value.status == -3
+    ni = g.nindex.copy()
+    ni[10] = g.edges + 100  # row beyond the edge array
+    with pytest.raises(E.EclError) as ei:
+        ctx.run_host(E.Graph(ni, g.nlist, g.eweight))
+    assert ei.value.status == -3
+    got, _ = ctx.run_host(g)  # the context stays usable
+    want, _, _ = O.oracle_mst(g.nindex, g.nlist, g.eweight)
+    assert np.array_equal(got, want)
+
+
+def test_too_large_for_context(ctx):
+    small = E.Context(100, 100)
+    g = E.gen_grid(20, 20, 1, 100)
+    with pytest.raises(E.EclError) as ei:
+        small.run_host(g)
+    assert ei.value.status == -9
+    small.close()
+
+
+def test_stats_are_consistent(ctx):
+    g = E.gen_rmat(16, 16, 0.57, 0.19, 0.19, 2, 1 << 24)
+    _, st = ctx.run_host(g, E.make_opts(flags=E.FLAG_STATS))
+    assert st["filtered"] == 1 and st["rounds"][0] > 0 and st["rounds"][1] > 0
+    assert st["scan_kept"][0] == st["wl_in"][0][0]
+    assert st["atomics"] > 0
+    assert st["ms_total"] > 0
+    assert st["forest_edges"] <= g.nodes - 1
+
+
+@pytest.mark.slow
+def test_rmat22_full_size_vs_oracle(ctx):
+    """The single-graph benchmark input (RMAT scale 22, edge factor 16, seed 2)."""
+    g = E.gen_rmat(22, 16, 0.57, 0.19, 0.19, 2, 1 << 24)
+    big = E.Context(g.nodes, g.edges)
+    t, f = E.heuristic_threshold(g)
+    want, w, fe = O.oracle_mst(g.nindex, g.nlist, g.eweight, t, f)
+    for kw in (dict(), dict(mode=E.THRESH_QUANTILE, quantile=0.05)):
+        got, st = big.run_host(g, E.make_opts(**kw))
+        assert np.array_equal(got, want), kw
+        assert st["forest_weight"] == w
+    big.close()
