@@ -41,6 +41,8 @@ WORKLOADS = {
     # name: (generator kwargs, description)
     "rmat22": ("rmat", dict(scale=22, edge_factor=16, seed=2, wmax=1 << 24),
                "RMAT scale 22, ef 16, a=.57 b=.19 c=.19, seed 2, w~U[1,2^24]"),
+    "rmat20": ("rmat", dict(scale=20, edge_factor=16, seed=2, wmax=1 << 24),
+               "RMAT scale 20, ef 16, a=.57 b=.19 c=.19, seed 2, w~U[1,2^24] (profiling size)"),
     "grid1000": ("grid", dict(rows=1000, cols=1000, seed=1, wmax=1_000_000),
                  "2D 4-neighbour grid 1000x1000, seed 1, w~U[1,1e6]"),
     "rmat25": ("rmat", dict(scale=25, edge_factor=16, seed=3, wmax=1 << 30),
@@ -208,6 +210,8 @@ def main():
     ap.add_argument("--split", type=int, default=0)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain ECL-MST comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--profile", action="store_true",
+                    help="device solves only (no e2e, plain or CPU legs): the command profiled by ncu")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -287,6 +291,13 @@ def main():
                              stream=stream.cuda_stream, stats=True)
     inmst = d_out[: g.edges].cpu().numpy()
     fw = int(g.eweight[inmst.astype(bool)].astype(np.int64).sum()) % 2**64
+
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"workload": args.workload, "ms_per_step": ms_step, "value": value,
+                              "rounds": last["rounds"], "forest_weight": fw}), flush=True)
+        ctx.close()
+        return
 
     # end to end through the C ABI with host buffers (pinned), H2D + solve + D2H per step
     h_ni = torch.from_numpy(g.nindex).pin_memory().numpy()

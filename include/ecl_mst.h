@@ -163,6 +163,9 @@ typedef struct ecl_mst_stats {
   float ms_total;          /* device time of the whole solve (CUDA events)      */
   float ms_rounds;         /* device time of the round kernels                  */
   float ms_scan;           /* device time of the scan kernels                   */
+  /* device-clock breakdown (microseconds) taken at the kernels' barriers:   */
+  float us_scan[2][3];     /* per scan: flatten, vertex pass, chunk pass        */
+  float us_round[2][ECL_MAX_ROUNDS][2]; /* per round: find/min pass, mark pass  */
 } ecl_mst_stats;
 
 /* ------------------------------------------------------------- the solve */

@@ -1,0 +1,672 @@
+// Kernels of the single-graph B200 ECL-MST engine.
+//
+// Replaces gpuMST<filter>'s kernels (ECL-MST/ECL_MST.cu): initPM (:147-154),
+// initWL<first> (:157-207), kernel1 (:210-226), kernel2 (:229-240),
+// kernel3 (:243-251), find (:127-134), join (:137-144). The answer is the
+// reference's: the unique minimum spanning forest under the strict order
+// (uint32 weight, CSR index j) over the one-direction entries nlist[j] > v,
+// built in a light phase (w <= threshold, signed compare as at :172) and a
+// heavy phase (w > threshold). Launch sequence of one solve:
+//
+//   k_prep        initPM + CSR checks + threshold choice + the tile->vertex
+//                 table of the edge-balanced scans
+//   k_scan<L,E>   initWL<true>: every thread takes E consecutive CSR entries
+//                 (128-bit loads); rows shorter than E stay inside one
+//                 thread, longer rows are spread over threads, warps and CTAs
+//                 (the reference's thread/warp degree split, :167/:185,
+//                 becomes the entries-per-thread E). Also zeroes inMST.
+//                 Appends are CTA-aggregated: one atomic per tile.
+//   k_rounds      all Boruvka rounds of the phase in one cooperative launch
+//                 (kernel1, kernel2, kernel3 per round, bounded grid
+//                 barriers, no host round trip per round).
+//   k_flatten     parent[v] = root(v) once after the light phase
+//   k_scan<H,E>   initWL<false>: keeps heavy entries across light trees
+//   k_rounds      heavy phase
+#pragma once
+#include <cuda_runtime.h>
+#include <climits>
+#include <stdint.h>
+
+#include "ecl_mst.h"
+#include "internal.h"
+#include "mst_kernels.cuh"
+
+namespace ecl {
+
+constexpr int kThreads = 512;          // threads of every engine kernel
+constexpr int kGran = kThreads * 4;    // entries per tile->vertex table step
+constexpr int kSegCap = 4096;          // vertices of a tile's nindex slice kept in smem
+#ifndef ECL_ROUND_EPT
+#define ECL_ROUND_EPT 4
+#endif
+#ifndef ECL_ROUND_MIN_BLOCKS
+#define ECL_ROUND_MIN_BLOCKS 1
+#endif
+constexpr int kEPT = ECL_ROUND_EPT;    // worklist entries per thread in a round tile
+constexpr int kHotLog = 9;             // hot representative table: 512 slots
+constexpr int kHotSlots = 1 << kHotLog;
+constexpr int kFindLog = 10;           // find cache: 1024 slots
+constexpr int kFindSlots = 1 << kFindLog;
+constexpr unsigned long long kBarrierTimeoutNs = 5ull * 1000 * 1000 * 1000;
+
+// Entries per thread of the edge-balanced scan for a degree split: rows
+// shorter than the split stay inside one thread.
+__host__ __device__ __forceinline__ int scan_ept(int split) {
+  return split <= 4 ? 4 : (split <= 8 ? 8 : 16);
+}
+
+struct PrepArgs {
+  int nodes, edges;
+  const int* nindex;
+  const int* eweight;
+  int* parent;
+  u64* minv0;
+  u64* minv1;
+  int* first_v;  // [tiles + 1]: vertex holding entry t * kGran; last = nodes - 1
+  int tiles;     // ceil(edges / kGran)
+  int mode, explicit_thr, split;
+  float quantile;
+  DevState* st;
+};
+
+struct ScanArgs {
+  int nodes, edges;
+  const int* nindex;
+  const int* nlist;
+  const int* eweight;
+  const int* first_v;
+  int tiles;
+  int* parent;
+  int4* wl;
+  unsigned wl_cap;
+  unsigned char* inMST;
+  int vec_ok;    // nlist / eweight 16-byte aligned
+  int zero_vec;  // inMST 16-byte aligned
+  DevState* st;
+};
+
+struct RoundArgs {
+  int phase;
+  int nodes;
+  int4* wl0;
+  int4* wl1;
+  unsigned wl_cap;
+  int* parent;
+  u64* minv0;
+  u64* minv1;
+  unsigned char* inMST;
+  DevState* st;
+  unsigned small_tail;
+  int count_atomics;
+};
+
+// ------------------------------------------------------------------ prep
+// Threshold rule, by mode (run by one CTA). HEURISTIC restates main's rule
+// (ECL_MST.cu:408,432-440); QUANTILE takes a quantile of a 4096-entry hashed
+// sample; LEARNED reads the quantile and split the MLP wrote into `st`.
+__device__ void choose_threshold(const PrepArgs& a, int* samp) {
+  DevState* st = a.st;
+  const int tid = threadIdx.x;
+  int mode = a.mode, split = a.split;
+  float quantile = a.quantile;
+  if (mode == ECL_THRESH_LEARNED) {
+    quantile = st->quantile;
+    split = st->learned_split;
+    mode = ECL_THRESH_QUANTILE;
+  }
+  const int nodes = a.nodes, edges = a.edges;
+  if (tid == 0) st->split = split;
+  if (mode == ECL_THRESH_NONE || (mode == ECL_THRESH_QUANTILE && !(quantile < 1.0f))) {
+    if (tid == 0) {
+      st->filtered = 0;
+      st->threshold = INT_MAX;
+    }
+    return;
+  }
+  if (mode == ECL_THRESH_EXPLICIT) {
+    if (tid == 0) {
+      st->filtered = 1;
+      st->threshold = a.explicit_thr;
+    }
+    return;
+  }
+  if (mode == ECL_THRESH_HEURISTIC) {
+    if (tid == 0) {
+      if (edges / nodes < 4) {
+        st->filtered = 0;
+        st->threshold = INT_MAX;
+      } else {
+        int s[20];
+        const int ns = edges < 20 ? edges : 20;
+        for (int i = 0; i < ns; i++) {
+          unsigned val = (unsigned)i;
+          val = ((val >> 16) ^ val) * 0x45d9f3bu;
+          val = ((val >> 16) ^ val) * 0x45d9f3bu;
+          val = (val >> 16) ^ val;
+          s[i] = a.eweight[val % (unsigned)edges];
+        }
+        for (int i = 1; i < ns; i++) {
+          const int x = s[i];
+          int k = i - 1;
+          while (k >= 0 && s[k] > x) {
+            s[k + 1] = s[k];
+            k--;
+          }
+          s[k + 1] = x;
+        }
+        st->filtered = 1;
+        st->threshold = s[min(19, (int)(3.0 * nodes * ns / edges))];
+      }
+    }
+    return;
+  }
+  const int S = 4096;
+  for (int i = tid; i < S; i += blockDim.x) {
+    const uint64_t r = ecl_mix64(0x5EED0000ull + (uint64_t)i);
+    samp[i] = a.eweight[(unsigned)(r % (uint64_t)(unsigned)edges)];
+  }
+  __syncthreads();
+  for (int k = 2; k <= S; k <<= 1) {  // bitonic sort in shared memory
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < S; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const int x = samp[i], y = samp[ixj];
+          if ((x > y) == ((i & k) == 0)) {
+            samp[i] = y;
+            samp[ixj] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0) {
+    const float q = quantile < 0.f ? 0.f : quantile;
+    int idx = (int)(q * (float)(S - 1));
+    idx = idx < 0 ? 0 : (idx > S - 1 ? S - 1 : idx);
+    st->filtered = 1;
+    st->threshold = samp[idx];
+  }
+}
+
+// Largest v in [0, nodes) with nindex[v] <= e (bounded even on bad input).
+__device__ __forceinline__ int vertex_of(const int* nindex, int nodes, long long e) {
+  int lo = 0, hi = nodes;  // invariant: nindex[lo] <= e (for a valid CSR), answer in [lo, hi)
+  while (hi - lo > 1) {
+    const int mid = lo + ((hi - lo) >> 1);
+    if ((long long)__ldg(nindex + mid) <= e) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kThreads) k_prep(PrepArgs a) {
+  __shared__ int samp[4096];
+  DevState* st = a.st;
+  if (blockIdx.x == 0) choose_threshold(a, samp);
+  const int n = a.nodes, m = a.edges;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  bool bad = false;
+  for (int v = gid; v < n; v += stride) {
+    a.parent[v] = v;
+    a.minv0[v] = kNoEdge;
+    a.minv1[v] = kNoEdge;
+    const int b = __ldg(a.nindex + v), e = __ldg(a.nindex + v + 1);
+    bad |= b < 0 || e < b || e > m;
+  }
+  if (gid == 0) bad |= __ldg(a.nindex) != 0 || __ldg(a.nindex + n) != m;
+  if (bad) atomicOr(&st->error, kErrFormat);
+  for (int t = gid; t <= a.tiles; t += stride)
+    a.first_v[t] = t < a.tiles ? vertex_of(a.nindex, n, (long long)t * kGran) : n - 1;
+}
+
+// ------------------------------------------------------------------ scans
+enum ScanKind { kLight = 0, kHeavy = 1 };
+
+// Edge-balanced CSR scan (initWL, ECL_MST.cu:157-207). Tile = kThreads * EPT
+// consecutive entries; thread t owns entries [tile0 + t*EPT, +EPT). The
+// vertex of each entry comes from the tile's slice of nindex in shared memory
+// (found through first_v), so hub rows and short rows cost the same per
+// entry. One-direction entries (nlist[j] > v) with the phase's weight test
+// are appended as {rep(v), rep(n), w, j}; the heavy scan additionally drops
+// entries whose endpoints share a light-phase tree (parent[] is flat, so a
+// rep is one load).
+template <int KIND, int EPT>
+__global__ void __launch_bounds__(kThreads) k_scan(ScanArgs a) {
+  __shared__ int sidx[kSegCap + 1];
+  __shared__ ReserveSmem sm;
+  DevState* st = a.st;
+  if (ld_volatile(&st->error) & kErrFormat) return;  // set by k_prep only
+  if (KIND == kHeavy && !st->filtered) return;
+  if (scan_ept(st->split) != EPT) return;  // only the variant the split selects runs
+  const int thr = st->threshold;
+  const int n = a.nodes, m = a.edges;
+  constexpr int kTile = kThreads * EPT;
+  constexpr int kStep = EPT / 4;  // first_v entries per tile
+  const long long e0 = (long long)blockIdx.x * kTile;
+  if (e0 >= m) return;
+  const int tb = blockIdx.x * kStep;
+  const int v_lo = __ldg(a.first_v + tb);
+  const int v_hi = __ldg(a.first_v + min(tb + kStep, a.tiles));
+  const int span = v_hi - v_lo + 1;  // vertices whose rows may hold this tile's entries
+  const bool seg = span <= kSegCap;
+  if (seg)
+    for (int i = threadIdx.x; i <= span; i += blockDim.x) sidx[i] = __ldg(a.nindex + v_lo + i);
+  __syncthreads();
+  auto row_start = [&](int i) -> int {  // nindex[v_lo + i]
+    return seg ? sidx[i] : __ldg(a.nindex + v_lo + i);
+  };
+
+  const long long j0 = e0 + (long long)threadIdx.x * EPT;
+  int nb[EPT], w[EPT];
+  if (j0 + EPT <= m && a.vec_ok) {
+#pragma unroll
+    for (int q = 0; q < EPT; q += 4) {
+      const int4 x = __ldg(reinterpret_cast<const int4*>(a.nlist + j0 + q));
+      const int4 y = __ldg(reinterpret_cast<const int4*>(a.eweight + j0 + q));
+      nb[q] = x.x; nb[q + 1] = x.y; nb[q + 2] = x.z; nb[q + 3] = x.w;
+      w[q] = y.x; w[q + 1] = y.y; w[q + 2] = y.z; w[q + 3] = y.w;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < EPT; q++) {
+      const bool in = j0 + q < m;
+      nb[q] = in ? __ldg(a.nlist + j0 + q) : -1;
+      w[q] = in ? __ldg(a.eweight + j0 + q) : 0;
+    }
+  }
+  if (KIND == kLight && j0 < m) {  // inMST = 0 (the reference memsets it, :306)
+    if (a.zero_vec && j0 + EPT <= m) {
+      if (EPT == 4) *reinterpret_cast<unsigned*>(a.inMST + j0) = 0u;
+      else if (EPT == 8) *reinterpret_cast<uint2*>(a.inMST + j0) = make_uint2(0u, 0u);
+      else *reinterpret_cast<uint4*>(a.inMST + j0) = make_uint4(0u, 0u, 0u, 0u);
+    } else {
+      for (int q = 0; q < EPT && j0 + q < m; q++) a.inMST[j0 + q] = 0;
+    }
+  }
+  // vertex of entry j0: the last i in [0, span) with row_start(i) <= j0
+  int i = 0;
+  if (j0 < m) {
+    int lo = 0, hi = span;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (row_start(mid) <= j0) lo = mid;
+      else hi = mid;
+    }
+    i = lo;
+  }
+  int row_end = row_start(i + 1);
+  int vtx[EPT], nrep[EPT];
+  unsigned keep = 0, cnt = 0;
+  int cur_v = -1, cur_rep = -1;
+#pragma unroll
+  for (int q = 0; q < EPT; q++) {
+    const long long j = j0 + q;
+    vtx[q] = 0;
+    nrep[q] = nb[q];
+    if (j >= m) continue;
+    while (j >= row_end && i < span - 1) {  // skip to the row holding j (zero-degree rows too)
+      i++;
+      row_end = row_start(i + 1);
+    }
+    const int v = v_lo + i;
+    if ((unsigned)nb[q] >= (unsigned)n) {
+      atomicOr(&st->error, kErrFormat);
+      continue;
+    }
+    if (nb[q] <= v) continue;
+    if (KIND == kLight ? !(w[q] <= thr) : !(w[q] > thr)) continue;
+    int rv = v;
+    if (KIND == kHeavy) {
+      if (v != cur_v) {
+        cur_v = v;
+        cur_rep = __ldg(a.parent + v);
+      }
+      rv = cur_rep;
+      nrep[q] = __ldg(a.parent + nb[q]);
+      if (nrep[q] == rv) continue;
+    }
+    vtx[q] = rv;
+    keep |= 1u << q;
+    cnt++;
+  }
+  unsigned pos, unused;
+  cta_reserve2(cnt, 0u, &st->wl_count[KIND][0], nullptr, sm, pos, unused);
+#pragma unroll
+  for (int q = 0; q < EPT; q++) {
+    if (!(keep & (1u << q))) continue;
+    if (pos < a.wl_cap) a.wl[pos] = make_int4(vtx[q], nrep[q], w[q], (int)(j0 + q));
+    else atomicOr(&st->error, kErrOverflow);
+    pos++;
+  }
+}
+
+// parent[v] = root(v) for every vertex, once before the heavy scan.
+__global__ void __launch_bounds__(kThreads) k_flatten(int* parent, int n, const DevState* st) {
+  if (!st->filtered || (ld_volatile(&st->error) & (kErrFormat | kErrTimeout))) return;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    __stcg(parent + v, find_ro(v, parent));
+}
+
+// ----------------------------------------------------------------- rounds
+// Per-CTA shared-memory state of the round kernel. Representatives shared by
+// many worklist entries (a growing giant component) would otherwise put
+// every entry's parent read, min-slot guard read, atomicMin and reset on one
+// L2 address; these small direct-mapped tables absorb the repeats per CTA.
+struct RoundSmem {
+  ReserveSmem rs;
+  int hot_rep[kHotSlots];    // hot representative -> CTA-local partial minimum
+  u64 hot_key[kHotSlots];
+  int reset_seen[kHotSlots]; // previous-round slots this CTA already cleared
+  u64 find_cache[kFindSlots];// (vertex << 32) | root, valid within one pass
+};
+
+__device__ __forceinline__ unsigned hot_slot(int r) { return ((unsigned)r * 0x9E3779B1u) >> (32 - kHotLog); }
+__device__ __forceinline__ unsigned find_slot(int r) { return ((unsigned)r * 0x85EBCA6Bu) >> (32 - kFindLog); }
+
+__device__ __forceinline__ void round_smem_clear(RoundSmem& s) {
+  for (int i = threadIdx.x; i < kHotSlots; i += blockDim.x) {
+    s.hot_rep[i] = -1;
+    s.hot_key[i] = kNoEdge;
+    s.reset_seen[i] = -1;
+  }
+  for (int i = threadIdx.x; i < kFindSlots; i += blockDim.x) s.find_cache[i] = kNoEdge;
+}
+
+// Roots of the 2*kEPT endpoints a thread holds, all walks advanced in lock
+// step so their loads are in flight together. A per-CTA cache of
+// (vertex << 32 | root) absorbs repeated endpoints (roots do not change
+// during the find/min pass). Path splitting re-points each visited node to
+// its grandparent (stays inside the tree; bounds long hook chains).
+template <int N>
+__device__ __forceinline__ void multi_find(int (&v)[N], const bool (&valid)[N], int* parent,
+                                           RoundSmem& s) {
+  int par[N];
+  unsigned miss = 0;
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    par[i] = v[i];
+    if (!valid[i]) continue;
+    const u64 c = ((volatile u64*)s.find_cache)[find_slot(v[i])];
+#ifdef ECL_NO_FINDCACHE
+    if (false) {
+#else
+    if ((int)(c >> 32) == v[i] && c != kNoEdge) {
+#endif
+      v[i] = (int)(unsigned)c;
+      par[i] = v[i];
+    } else {
+      miss |= 1u << i;
+      par[i] = __ldcg(parent + v[i]);
+    }
+  }
+  int orig[N];
+#pragma unroll
+  for (int i = 0; i < N; i++) orig[i] = v[i];
+  for (;;) {
+    int gp[N];
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+      gp[i] = par[i];
+      if (par[i] != v[i]) {
+        any = true;
+        gp[i] = __ldcg(parent + par[i]);
+      }
+    }
+    if (!any) break;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+      if (par[i] != v[i]) {
+#ifndef ECL_NO_SPLIT
+        if (gp[i] != par[i]) __stcg(parent + v[i], gp[i]);
+#endif
+        v[i] = par[i];
+        par[i] = gp[i];
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < N; i++)
+    if (miss & (1u << i))
+      ((volatile u64*)s.find_cache)[find_slot(orig[i])] = ((u64)(unsigned)orig[i] << 32) | (unsigned)v[i];
+}
+
+// Clear a previous-round min slot once per CTA.
+__device__ __forceinline__ void reset_prev(int r, u64* mprev, RoundSmem& s) {
+  const unsigned slot = hot_slot(r);
+  if (((volatile int*)s.reset_seen)[slot] == r) return;
+  ((volatile int*)s.reset_seen)[slot] = r;
+  __stcg(mprev + r, kNoEdge);
+}
+
+// Offer each of a thread's N (rep, key) pairs to the rep's min slot: the
+// guarded atomicMin of ECL_MST.cu:221-223. Lanes of a warp holding the same
+// rep first reduce to the group minimum (warp-cooperative for high-degree
+// representatives); a group leader then folds it into the CTA's hot table.
+// Singletons, and leaders whose table slot belongs to another rep, read the
+// global slots together (one round trip for all pairs) and issue
+// fire-and-forget atomicMin only where the guard shows an improvement.
+// Every lane of the warp must call this.
+template <int N>
+__device__ __forceinline__ void offer_mins(const int (&rep)[N], const u64 (&key)[N],
+                                           const bool (&valid)[N], u64* mcur, RoundSmem& s,
+                                           unsigned long long& atomics) {
+  const int lane = threadIdx.x & 31;
+  bool cold[N];
+  u64 val[N];
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    const unsigned g = __match_any_sync(0xffffffffu, valid[i] ? rep[i] : -2 - lane);
+    cold[i] = false;
+    val[i] = key[i];
+    if (!valid[i]) continue;
+#ifdef ECL_NO_HOT
+    if (true) {
+#else
+    if ((g & (g - 1)) == 0) {
+#endif
+      cold[i] = true;
+      continue;
+    }
+    const unsigned khi = (unsigned)(key[i] >> 32);
+    const unsigned hi = __reduce_min_sync(g, khi);
+    const unsigned lo = __reduce_min_sync(g, khi == hi ? (unsigned)key[i] : 0xffffffffu);
+    if (lane != __ffs(g) - 1) continue;
+    const u64 gm = ((u64)hi << 32) | lo;
+    const unsigned slot = hot_slot(rep[i]);
+    int cur = ((volatile int*)s.hot_rep)[slot];
+    if (cur < 0) {
+      cur = atomicCAS(&s.hot_rep[slot], -1, rep[i]);
+      if (cur < 0) cur = rep[i];
+    }
+    if (cur == rep[i]) {
+      if (((volatile u64*)s.hot_key)[slot] > gm) atomicMin(&s.hot_key[slot], gm);
+    } else {
+      cold[i] = true;
+      val[i] = gm;
+    }
+  }
+  u64 seen[N];
+#pragma unroll
+  for (int i = 0; i < N; i++) seen[i] = cold[i] ? __ldcg(mcur + rep[i]) : 0ull;
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    if (cold[i] && seen[i] > val[i]) {
+      atomicMin(mcur + rep[i], val[i]);
+      atomics++;
+    }
+  }
+}
+
+// kernel1 (ECL_MST.cu:210-226) plus kernel3 of the previous round (:243-251):
+// each input entry clears its endpoints' slots in the previous round's min
+// array, resolves its endpoints to reps, and if they differ is compacted into
+// `out` with the reps (implicit path compression, :218-219) and offers its
+// key to both reps' min slots.
+__device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* in, unsigned W,
+                                               int4* out, unsigned* out_ctr, u64* mcur, u64* mprev,
+                                               bool reset, unsigned start, unsigned stride,
+                                               RoundSmem& s) {
+  constexpr int N = 2 * kEPT;
+  const unsigned tile = blockDim.x * kEPT;
+  const unsigned ntiles = (W + tile - 1) / tile;
+  unsigned long long atomics = 0;
+  for (unsigned t = start; t < ntiles; t += stride) {
+    int4 e[kEPT];
+    bool in_range[kEPT];
+#pragma unroll
+    for (int k = 0; k < kEPT; k++) {
+      const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
+      in_range[k] = idx < W;
+      e[k] = in_range[k] ? __ldcg(in + idx) : make_int4(0, 0, 0, 0);
+    }
+    int v[N];
+    bool vv[N];
+#pragma unroll
+    for (int k = 0; k < kEPT; k++) {
+      v[2 * k] = e[k].x;
+      v[2 * k + 1] = e[k].y;
+      vv[2 * k] = vv[2 * k + 1] = in_range[k];
+      if (reset && in_range[k]) {
+        reset_prev(e[k].x, mprev, s);
+        reset_prev(e[k].y, mprev, s);
+      }
+    }
+    multi_find<N>(v, vv, a.parent, s);
+    bool keep[kEPT];
+    unsigned cnt = 0;
+#pragma unroll
+    for (int k = 0; k < kEPT; k++) {
+      keep[k] = in_range[k] && v[2 * k] != v[2 * k + 1];
+      e[k].x = v[2 * k];
+      e[k].y = v[2 * k + 1];
+      cnt += keep[k];
+    }
+    unsigned pos, unused;
+    cta_reserve2(cnt, 0u, out_ctr, nullptr, s.rs, pos, unused);
+    u64 key[N];
+    bool kv[N];
+#pragma unroll
+    for (int k = 0; k < kEPT; k++) {
+      if (keep[k]) {
+        if (pos < a.wl_cap) out[pos] = e[k];
+        else atomicOr(&a.st->error, kErrOverflow);
+        pos++;
+      }
+      key[2 * k] = key[2 * k + 1] = edge_key(e[k].z, e[k].w);
+      kv[2 * k] = kv[2 * k + 1] = keep[k];
+    }
+    offer_mins<N>(v, key, kv, mcur, s, atomics);
+  }
+  __syncthreads();
+  // flush the CTA's partial minima of hot representatives
+  for (int i = threadIdx.x; i < kHotSlots; i += blockDim.x) {
+    const int r = s.hot_rep[i];
+    if (r >= 0) {
+      const u64 k = s.hot_key[i];
+      if (__ldcg(mcur + r) > k) {
+        atomicMin(mcur + r, k);
+        atomics++;
+      }
+    }
+  }
+  if (a.count_atomics && atomics) atomicAdd(&a.st->atomics, atomics);
+}
+
+// After the barrier: the hot table's reps now read their final minima.
+__device__ __forceinline__ void hot_refresh(const u64* mcur, RoundSmem& s) {
+  for (int i = threadIdx.x; i < kHotSlots; i += blockDim.x) {
+    const int r = s.hot_rep[i];
+    if (r >= 0) s.hot_key[i] = __ldcg(mcur + r);
+  }
+  __syncthreads();
+}
+
+// kernel2 (ECL_MST.cu:229-240): an entry whose key is the minimum of either
+// endpoint's slot is a forest edge: union the trees and mark inMST[j].
+__device__ __forceinline__ void round_mark(const RoundArgs& a, const int4* wl, unsigned W,
+                                           const u64* mcur, unsigned start, unsigned stride,
+                                           const RoundSmem& s) {
+  const unsigned tile = blockDim.x * kEPT;
+  const unsigned ntiles = (W + tile - 1) / tile;
+  for (unsigned t = start; t < ntiles; t += stride) {
+    int4 e[kEPT];
+    bool in_range[kEPT];
+#pragma unroll
+    for (int k = 0; k < kEPT; k++) {
+      const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
+      in_range[k] = idx < W;
+      e[k] = in_range[k] ? __ldcg(wl + idx) : make_int4(0, 0, 0, 0);
+    }
+    u64 mx[kEPT], my[kEPT];
+#pragma unroll
+    for (int k = 0; k < kEPT; k++) {
+      mx[k] = my[k] = kNoEdge;
+      if (!in_range[k]) continue;
+      const unsigned sx = hot_slot(e[k].x), sy = hot_slot(e[k].y);
+      mx[k] = s.hot_rep[sx] == e[k].x ? s.hot_key[sx] : __ldcg(mcur + e[k].x);
+      my[k] = s.hot_rep[sy] == e[k].y ? s.hot_key[sy] : __ldcg(mcur + e[k].y);
+    }
+#pragma unroll
+    for (int k = 0; k < kEPT; k++) {
+      if (!in_range[k]) continue;
+      const u64 key = edge_key(e[k].z, e[k].w);
+      if (key == mx[k] || key == my[k]) {
+        cas_union(e[k].x, e[k].y, a.parent);
+        a.inMST[e[k].w] = 1;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(RoundArgs a) {
+  __shared__ RoundSmem s;
+  DevState* st = a.st;
+  const int ph = a.phase;
+  if (ph == 1 && !st->filtered) return;
+  // Only bits no CTA of this kernel can set, so every CTA takes the same exit.
+  if (ld_volatile(&st->error) & (kErrFormat | kErrTimeout)) return;
+  round_smem_clear(s);
+  __syncthreads();
+  bool tail = false;
+  int r = 0;
+  const bool stamp = blockIdx.x == 0 && threadIdx.x == 0;
+  if (stamp) st->t_round_start[ph] = globaltimer_ns();
+  for (;;) {
+    const unsigned W = min(ld_volatile(&st->wl_count[ph][r]), a.wl_cap);
+    if (W == 0) break;
+    if (r >= ECL_MAX_ROUNDS) {
+      if (stamp) atomicOr(&st->error, kErrRounds);
+      break;
+    }
+    if (!tail && W <= a.small_tail) {
+      tail = true;
+      if (blockIdx.x != 0) return;
+    }
+    const unsigned start = tail ? 0u : blockIdx.x, stride = tail ? 1u : gridDim.x;
+    const bool odd = (r & 1) != 0;
+    const int4* in = odd ? a.wl1 : a.wl0;
+    int4* out = odd ? a.wl0 : a.wl1;
+    u64* mcur = odd ? a.minv1 : a.minv0;
+    u64* mprev = odd ? a.minv0 : a.minv1;
+    round_find_min(a, in, W, out, &st->wl_count[ph][r + 1], mcur, mprev, r > 0, start, stride, s);
+    if (tail) __syncthreads();
+    else if (!grid_barrier(st, kBarrierTimeoutNs)) return;
+    if (stamp) st->t_round[ph][2 * r] = globaltimer_ns();
+    const unsigned W2 = min(ld_volatile(&st->wl_count[ph][r + 1]), a.wl_cap);
+    r++;
+    if (W2 == 0) break;
+    hot_refresh(mcur, s);
+    round_mark(a, out, W2, mcur, start, stride, s);
+    __syncthreads();
+    round_smem_clear(s);
+    if (tail) __syncthreads();
+    else if (!grid_barrier(st, kBarrierTimeoutNs)) return;
+    if (stamp) st->t_round[ph][2 * r - 1] = globaltimer_ns();
+  }
+  if (stamp) st->rounds[ph] = r;
+}
+
+}  // namespace ecl

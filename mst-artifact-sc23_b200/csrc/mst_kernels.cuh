@@ -39,6 +39,11 @@ struct DevState {
   int learned_split;   // learned mode: predicted degree split
   u64 atomics;         // guarded atomicMin issued (stats mode)
   unsigned wl_count[2][ECL_MAX_ROUNDS + 1];  // [phase][r] = entries entering round r
+  // globaltimer stamps taken by CTA 0 at phase boundaries (diagnostics):
+  // [phase][2r] after round r's find/min pass, [phase][2r+1] after its mark pass
+  u64 t_round_start[2];
+  u64 t_round[2][2 * ECL_MAX_ROUNDS];
+  u64 t_scan[2][4];  // start, after flatten, after pass 1, after pass 2
 };
 
 __device__ __forceinline__ u64 globaltimer_ns() {

@@ -18,7 +18,7 @@ from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_int64
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libecl_mst.so")
+LIB_PATH = os.environ.get("ECL_MST_LIB") or os.path.join(_HERE, "libecl_mst.so")
 
 ECL_OK = 0
 STATUS = {
@@ -54,7 +54,8 @@ class MstStats(ctypes.Structure):
                 ("rounds", c_int32 * 2), ("status", c_int32), ("scan_kept", c_int64 * 2),
                 ("wl_in", (c_int64 * MAX_ROUNDS) * 2), ("atomics", c_int64),
                 ("forest_edges", c_int64), ("forest_weight", c_uint64),
-                ("ms_total", c_float), ("ms_rounds", c_float), ("ms_scan", c_float)]
+                ("ms_total", c_float), ("ms_rounds", c_float), ("ms_scan", c_float),
+                ("us_scan", (c_float * 3) * 2), ("us_round", ((c_float * 2) * MAX_ROUNDS) * 2)]
 
     def as_dict(self):
         return {
@@ -65,6 +66,8 @@ class MstStats(ctypes.Structure):
             "atomics": self.atomics, "forest_edges": self.forest_edges,
             "forest_weight": self.forest_weight, "ms_total": self.ms_total,
             "ms_rounds": self.ms_rounds, "ms_scan": self.ms_scan,
+            "us_scan": [list(self.us_scan[p]) for p in range(2)],
+            "us_round": [[list(self.us_round[p][r]) for r in range(max(self.rounds[p], 0))] for p in range(2)],
         }
 
 
