@@ -37,16 +37,19 @@ constexpr int kThreads = 512;          // threads of every engine kernel
 constexpr int kGran = kThreads * 4;    // entries per tile->vertex table step
 constexpr int kSegCap = 4096;          // vertices of a tile's nindex slice kept in smem
 #ifndef ECL_ROUND_EPT
-#define ECL_ROUND_EPT 4
+#define ECL_ROUND_EPT 1
 #endif
 #ifndef ECL_ROUND_MIN_BLOCKS
-#define ECL_ROUND_MIN_BLOCKS 1
+#define ECL_ROUND_MIN_BLOCKS 4
 #endif
 constexpr int kEPT = ECL_ROUND_EPT;    // worklist entries per thread in a round tile
 constexpr int kHotLog = 9;             // hot representative table: 512 slots
 constexpr int kHotSlots = 1 << kHotLog;
 constexpr int kFindLog = 10;           // find cache: 1024 slots
 constexpr int kFindSlots = 1 << kFindLog;
+constexpr int kPairLog = 10;           // parallel-edge table: 1024 slots
+constexpr int kPairSlots = 1 << kPairLog;
+constexpr u64 kNoPair = ~0ull;
 constexpr unsigned long long kBarrierTimeoutNs = 5ull * 1000 * 1000 * 1000;
 
 // Entries per thread of the edge-balanced scan for a degree split: rows
@@ -360,6 +363,8 @@ struct RoundSmem {
   u64 hot_key[kHotSlots];
   int reset_seen[kHotSlots]; // previous-round slots this CTA already cleared
   u64 find_cache[kFindSlots];// (vertex << 32) | root, valid within one pass
+  u64 pair_tag[kPairSlots];  // (lo rep << 32) | hi rep of a tile's cross entry
+  u64 pair_min[kPairSlots];  // smallest key of that rep pair within the tile
 };
 
 __device__ __forceinline__ unsigned hot_slot(int r) { return ((unsigned)r * 0x9E3779B1u) >> (32 - kHotLog); }
@@ -372,6 +377,65 @@ __device__ __forceinline__ void round_smem_clear(RoundSmem& s) {
     s.reset_seen[i] = -1;
   }
   for (int i = threadIdx.x; i < kFindSlots; i += blockDim.x) s.find_cache[i] = kNoEdge;
+  for (int i = threadIdx.x; i < kPairSlots; i += blockDim.x) {
+    s.pair_tag[i] = kNoPair;
+    s.pair_min[i] = kNoEdge;
+  }
+}
+
+__device__ __forceinline__ unsigned pair_slot(u64 pk) {
+  return (unsigned)((pk * 0x9E3779B97F4A7C15ull) >> (64 - kPairLog));
+}
+
+// Parallel-edge elimination in the contracted graph. Entries of one tile
+// that join the same two trees are parallel edges of the contracted graph;
+// only the one with the smallest (weight, j) key can be a forest edge (any
+// forest through a heavier one is heavier than the same forest through the
+// lightest), so the others are dropped for good. Warp groups with equal rep
+// pairs reduce first; group minima meet in a per-tile shared table. keep[k]
+// is narrowed to the survivors. Every thread of the CTA must call this.
+template <int E>
+__device__ __forceinline__ void drop_parallel(const int4 (&e)[E], bool (&keep)[E], RoundSmem& s) {
+  const int lane = threadIdx.x & 31;
+  u64 pk[E], gmin[E];
+#pragma unroll
+  for (int k = 0; k < E; k++) {
+    const unsigned lo = (unsigned)min(e[k].x, e[k].y), hi = (unsigned)max(e[k].x, e[k].y);
+    pk[k] = keep[k] ? (((u64)lo << 32) | hi) : (0xFFFFFFFF00000000ull | (threadIdx.x * E + k));
+    const u64 key = edge_key(e[k].z, e[k].w);
+    const unsigned g = __match_any_sync(0xffffffffu, pk[k]);
+    gmin[k] = key;
+    if (!keep[k]) continue;
+    if (g & (g - 1)) {
+      const unsigned khi = (unsigned)(key >> 32);
+      const unsigned mhi = __reduce_min_sync(g, khi);
+      const unsigned mlo = __reduce_min_sync(g, khi == mhi ? (unsigned)key : 0xffffffffu);
+      gmin[k] = ((u64)mhi << 32) | mlo;
+    }
+    if (lane == __ffs(g) - 1) {
+      const unsigned slot = pair_slot(pk[k]);
+      u64 t = ((volatile u64*)s.pair_tag)[slot];
+      if (t == kNoPair) {
+        t = atomicCAS(&s.pair_tag[slot], kNoPair, pk[k]);
+        if (t == kNoPair) t = pk[k];
+      }
+      if (t == pk[k] && ((volatile u64*)s.pair_min)[slot] > gmin[k]) atomicMin(&s.pair_min[slot], gmin[k]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < E; k++) {
+    if (!keep[k]) continue;
+    const unsigned slot = pair_slot(pk[k]);
+    const u64 key = edge_key(e[k].z, e[k].w);
+    const u64 best = s.pair_tag[slot] == pk[k] ? s.pair_min[slot] : gmin[k];
+    keep[k] = key == best;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kPairSlots; i += blockDim.x) {
+    s.pair_tag[i] = kNoPair;
+    s.pair_min[i] = kNoEdge;
+  }
 }
 
 // Roots of the 2*kEPT endpoints a thread holds, all walks advanced in lock
@@ -542,8 +606,12 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
       keep[k] = in_range[k] && v[2 * k] != v[2 * k + 1];
       e[k].x = v[2 * k];
       e[k].y = v[2 * k + 1];
-      cnt += keep[k];
     }
+#ifndef ECL_NO_DEDUP
+    drop_parallel<kEPT>(e, keep, s);
+#endif
+#pragma unroll
+    for (int k = 0; k < kEPT; k++) cnt += keep[k];
     unsigned pos, unused;
     cta_reserve2(cnt, 0u, out_ctr, nullptr, s.rs, pos, unused);
     u64 key[N];
