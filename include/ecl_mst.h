@@ -197,6 +197,27 @@ int ecl_mst_run_device(ecl_mst_ctx* ctx, const ecl_graph* d_graph,
                        uint8_t* d_inMST, const mst_opts* opts, void* stream,
                        ecl_mst_stats* stats);
 
+/* Allocation-free device solve. This entry point has no counterpart in the
+ * reference; it exists for callers that must not allocate device memory
+ * (code running inside an allocator or memory-pool callback, embeddings that
+ * own every allocation of the process, services with a device-memory budget
+ * fixed at start-up). It calls no cudaMalloc, cudaFree or allocating library
+ * routine: its scratch is one file-scope device array of about 21 MB that
+ * every GPU loading this library holds until the process exits.
+ *   - d_graph holds DEVICE pointers, d_inMST a device buffer of edges bytes;
+ *   - limits: nodes <= 262,144 and edges <= 1,048,576, else ECL_ERR_TOO_LARGE;
+ *     at most edges/2 one-direction entries (nlist[j] > v), which every
+ *     symmetric input satisfies, else ECL_ERR_OVERFLOW;
+ *   - ECL_THRESH_LEARNED is not available here (ECL_ERR_UNSUPPORTED);
+ *   - the first call on a device resolves the scratch address on that device
+ *     (make it before any stream capture); the call enqueues on `stream`
+ *     (cudaStream_t, NULL = legacy default stream) and returns after the solve
+ *     finished, with device-side errors as its status;
+ *   - all calls share the one scratch array: calls that overlap on the GPU
+ *     (other threads, other streams) race and give wrong results. */
+int ecl_mst_run_device_noalloc(const ecl_graph* d_graph, uint8_t* d_inMST,
+                               const mst_opts* opts, void* stream);
+
 /* Wait for the context's stream and report a device-side error if any. */
 int ecl_mst_ctx_sync(ecl_mst_ctx* ctx);
 

@@ -422,3 +422,165 @@ extern "C" int ecl_host_alloc_pinned(size_t bytes, void** out) {
 extern "C" void ecl_host_free_pinned(void* p) {
   if (p) cudaFreeHost(p);
 }
+
+// ===================================================== allocation-free solve
+// Some callers cannot allocate device memory: code that runs inside a host
+// allocator hook or a memory-pool callback, an embedding that owns every
+// allocation of the process, or a service whose device memory budget is
+// fixed at start-up. ecl_mst_run_device_noalloc serves them: its scratch
+// (min slots, parent array, worklists, control block) is one file-scope
+// device array, created when the module loads and kept until the process
+// exits, on every GPU that loads this library. The caller passes only the
+// device CSR and the device inMST output.
+#include <mutex>
+
+namespace {
+
+constexpr int64_t kNaMaxNodes = 1 << 18;              // 262,144 vertices
+constexpr int64_t kNaMaxEdges = 1 << 20;              // 1,048,576 directed CSR entries
+constexpr int64_t kNaWlCap = kNaMaxEdges / 2;         // one-direction entries per worklist
+constexpr int64_t kNaTiles = kNaMaxEdges / kGran + 2; // tile -> vertex table entries
+
+constexpr size_t na_align(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t kNaOffState = 0;
+constexpr size_t kNaOffMinv0 = na_align(kNaOffState + sizeof(DevState));
+constexpr size_t kNaOffMinv1 = na_align(kNaOffMinv0 + sizeof(u64) * kNaMaxNodes);
+constexpr size_t kNaOffParent = na_align(kNaOffMinv1 + sizeof(u64) * kNaMaxNodes);
+constexpr size_t kNaOffFirstV = na_align(kNaOffParent + sizeof(int) * kNaMaxNodes);
+constexpr size_t kNaOffWl0 = na_align(kNaOffFirstV + sizeof(int) * kNaTiles);
+constexpr size_t kNaOffWl1 = na_align(kNaOffWl0 + sizeof(int4) * kNaWlCap);
+constexpr size_t kNaBytes = na_align(kNaOffWl1 + sizeof(int4) * kNaWlCap);  // about 21 MB
+
+// The scratch itself. In host code this name is only a stand-in for the
+// symbol, never a device address: the address comes from
+// cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_na_scratch[kNaBytes];
+
+struct NaDevice {
+  bool ready = false;
+  unsigned char* base = nullptr;  // device address of g_na_scratch on this device
+  int sm_count = 0;
+  int round_grid = 0;
+};
+constexpr int kNaMaxDevices = 64;
+NaDevice g_na_dev[kNaMaxDevices];
+std::mutex g_na_mu;
+
+// Once per device, with that device current: resolve the scratch address and
+// the cooperative grid size. No allocation happens here.
+int na_setup(int dev, NaDevice** out) {
+  if (dev < 0 || dev >= kNaMaxDevices) return ECL_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_na_mu);
+  NaDevice& d = g_na_dev[dev];
+  if (!d.ready) {
+    void* p = nullptr;
+    ECL_CUDA_TRY(cudaGetSymbolAddress(&p, g_na_scratch));
+    int coop = 0;
+    ECL_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) return ECL_ERR_UNSUPPORTED;
+    ECL_CUDA_TRY(cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev));
+    d.round_grid = coop_grid((const void*)k_rounds, kThreads, d.sm_count);
+    if (d.round_grid <= 0) return ECL_ERR_CUDA;
+    d.base = (unsigned char*)p;
+    d.ready = true;
+  }
+  *out = &d;
+  return ECL_OK;
+}
+
+}  // namespace
+
+extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
+                                          const mst_opts* opts, void* stream) {
+  if (!g || !d_inMST || g->nodes < 1 || g->edges < 0) return ECL_ERR_INVALID_ARG;
+  if (g->nodes > kNaMaxNodes || g->edges > kNaMaxEdges) return ECL_ERR_TOO_LARGE;
+  if (!g->nindex || (g->edges > 0 && (!g->nlist || !g->eweight))) return ECL_ERR_INVALID_ARG;
+  mst_opts o;
+  if (opts) o = *opts;
+  else ecl_default_opts(&o);
+  int st = check_opts(&o);
+  if (st) return st;
+  if (o.threshold_mode == ECL_THRESH_LEARNED) return ECL_ERR_UNSUPPORTED;
+  if (g->edges == 0) return ECL_OK;
+  int dev = 0;
+  ECL_CUDA_TRY(cudaGetDevice(&dev));
+  NaDevice* d = nullptr;
+  if ((st = na_setup(dev, &d))) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int n = g->nodes, m = g->edges;
+  DevState* dst = (DevState*)(d->base + kNaOffState);
+  int* parent = (int*)(d->base + kNaOffParent);
+  u64* minv0 = (u64*)(d->base + kNaOffMinv0);
+  u64* minv1 = (u64*)(d->base + kNaOffMinv1);
+  int* first_v = (int*)(d->base + kNaOffFirstV);
+  int4* wl0 = (int4*)(d->base + kNaOffWl0);
+  int4* wl1 = (int4*)(d->base + kNaOffWl1);
+  // The array keeps the previous call's contents: the control block (error
+  // word, worklist counters, barrier) must start at zero; k_prep initialises
+  // parent[] and both min arrays.
+  ECL_CUDA_TRY(cudaMemsetAsync(dst, 0, sizeof(DevState), s));
+  const int split = o.degree_split > 0 ? o.degree_split : kDefaultSplit;
+  const int tiles = (int)(((int64_t)m + kGran - 1) / kGran);
+  PrepArgs pa;
+  pa.nodes = n;
+  pa.edges = m;
+  pa.nindex = g->nindex;
+  pa.eweight = g->eweight;
+  pa.parent = parent;
+  pa.minv0 = minv0;
+  pa.minv1 = minv1;
+  pa.first_v = first_v;
+  pa.tiles = tiles;
+  pa.mode = o.threshold_mode;
+  pa.explicit_thr = o.threshold;
+  pa.split = split;
+  pa.quantile = o.quantile;
+  pa.st = dst;
+  const int64_t prep_items = std::max<int64_t>(n, (int64_t)tiles + 1);
+  const int prep_grid = (int)std::min<int64_t>((prep_items + kThreads - 1) / kThreads, (int64_t)d->sm_count * 16);
+  k_prep<<<std::max(prep_grid, 1), kThreads, 0, s>>>(pa);
+  ECL_CUDA_TRY(cudaGetLastError());
+  ScanArgs sa;
+  sa.nodes = n;
+  sa.edges = m;
+  sa.nindex = g->nindex;
+  sa.nlist = g->nlist;
+  sa.eweight = g->eweight;
+  sa.first_v = first_v;
+  sa.tiles = tiles;
+  sa.parent = parent;
+  sa.wl = wl0;
+  sa.wl_cap = (unsigned)kNaWlCap;
+  sa.inMST = d_inMST;
+  sa.vec_ok = ((((uintptr_t)g->nlist) | ((uintptr_t)g->eweight)) & 15) == 0;
+  sa.zero_vec = (((uintptr_t)d_inMST) & 15) == 0;
+  sa.st = dst;
+  RoundArgs ra;
+  ra.nodes = n;
+  ra.wl0 = wl0;
+  ra.wl1 = wl1;
+  ra.wl_cap = (unsigned)kNaWlCap;
+  ra.parent = parent;
+  ra.minv0 = minv0;
+  ra.minv1 = minv1;
+  ra.inMST = d_inMST;
+  ra.st = dst;
+  ra.small_tail = o.small_tail < 0 ? 0u : (o.small_tail == 0 ? kDefaultSmallTail : (unsigned)o.small_tail);
+  if (o.flags & ECL_FLAG_NO_SMALL_TAIL) ra.small_tail = 0;
+  ra.count_atomics = (o.flags & ECL_FLAG_STATS) ? 1 : 0;
+  const int rgrid = std::max(1, std::min(d->round_grid, (m / 2 + kThreads * kEPT - 1) / (kThreads * kEPT) + 1));
+  if ((st = launch_scan<kLight>(scan_ept(split), sa, s))) return st;
+  ra.phase = 0;
+  if ((st = launch_coop((const void*)k_rounds, rgrid, kThreads, &ra, s))) return st;
+  const int fgrid = (int)std::min<int64_t>(((int64_t)n + kThreads - 1) / kThreads, (int64_t)d->sm_count * 16);
+  k_flatten<<<std::max(fgrid, 1), kThreads, 0, s>>>(parent, n, dst);
+  ECL_CUDA_TRY(cudaGetLastError());
+  if ((st = launch_scan<kHeavy>(scan_ept(split), sa, s))) return st;
+  ra.phase = 1;
+  if ((st = launch_coop((const void*)k_rounds, rgrid, kThreads, &ra, s))) return st;
+  // Report device-side errors (malformed CSR, worklist overflow) to the caller.
+  unsigned err = 0;
+  ECL_CUDA_TRY(cudaMemcpyAsync(&err, &dst->error, sizeof(err), cudaMemcpyDeviceToHost, s));
+  ECL_CUDA_TRY(cudaStreamSynchronize(s));
+  return device_error_status(err);
+}

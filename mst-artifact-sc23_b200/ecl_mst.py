@@ -103,6 +103,7 @@ def load():
         "ecl_mst_ctx_run_host": (c_int, [c_void_p, G, c_void_p, POINTER(MstOpts), POINTER(MstStats)]),
         "ecl_mst_run_device": (c_int, [c_void_p, G, c_void_p, POINTER(MstOpts), c_void_p, POINTER(MstStats)]),
         "ecl_mst_ctx_sync": (c_int, [c_void_p]),
+        "ecl_mst_run_device_noalloc": (c_int, [G, c_void_p, POINTER(MstOpts), c_void_p]),
         "ecl_mst_ctx_stream": (c_void_p, [c_void_p]),
         "ecl_host_alloc_pinned": (c_int, [ctypes.c_size_t, POINTER(c_void_p)]),
         "ecl_host_free_pinned": (None, [c_void_p]),
@@ -231,6 +232,16 @@ def mst(g, opts=None):
     _check(load().ecl_mst_run(ctypes.byref(gs), _ptr(out), None if opts is None else ctypes.byref(opts),
                               ctypes.byref(st)), "ecl_mst_run")
     return out[: g.edges], st.as_dict()
+
+
+def run_device_noalloc(nodes, edges, d_nindex, d_nlist, d_eweight, d_inMST, opts=None, stream=None):
+    """Allocation-free solve (ecl_mst_run_device_noalloc): device pointers in
+    and out, scratch in the library's static device array; returns after the
+    solve. For callers that cannot allocate device memory."""
+    gs = EclGraphC(nodes, edges, d_nindex, d_nlist, d_eweight)
+    _check(load().ecl_mst_run_device_noalloc(ctypes.byref(gs), d_inMST,
+                                             None if opts is None else ctypes.byref(opts), stream),
+           "run_device_noalloc")
 
 
 def verify(g, a, b):
