@@ -175,10 +175,10 @@ int launch_coop(const void* fn, int grid, int threads, void* arg, cudaStream_t s
 template <int KIND>
 int launch_scan(int ept, const ScanArgs& sa, cudaStream_t s) {
   const int m = sa.edges;
-  const int blocks = (int)((m + (int64_t)kThreads * ept - 1) / ((int64_t)kThreads * ept));
-  if (ept == 4) k_scan<KIND, 4><<<blocks, kThreads, 0, s>>>(sa);
-  else if (ept == 8) k_scan<KIND, 8><<<blocks, kThreads, 0, s>>>(sa);
-  else k_scan<KIND, 16><<<blocks, kThreads, 0, s>>>(sa);
+  const int blocks = (int)((m + (int64_t)kScanThreads * ept - 1) / ((int64_t)kScanThreads * ept));
+  if (ept == 4) k_scan<KIND, 4><<<blocks, kScanThreads, 0, s>>>(sa);
+  else if (ept == 8) k_scan<KIND, 8><<<blocks, kScanThreads, 0, s>>>(sa);
+  else k_scan<KIND, 16><<<blocks, kScanThreads, 0, s>>>(sa);
   return cuda_status(cudaGetLastError());
 }
 

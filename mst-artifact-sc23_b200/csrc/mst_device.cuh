@@ -33,8 +33,9 @@
 
 namespace ecl {
 
-constexpr int kThreads = 512;          // threads of every engine kernel
-constexpr int kGran = kThreads * 4;    // entries per tile->vertex table step
+constexpr int kThreads = 512;          // threads of the prep, flatten and round kernels
+constexpr int kScanThreads = 256;      // threads of a scan CTA
+constexpr int kGran = kScanThreads * 4;// entries per tile->vertex table step
 constexpr int kSegCap = 4096;          // vertices of a tile's nindex slice kept in smem
 #ifndef ECL_ROUND_EPT
 #define ECL_ROUND_EPT 1
@@ -236,7 +237,7 @@ enum ScanKind { kLight = 0, kHeavy = 1 };
 // entries whose endpoints share a light-phase tree (parent[] is flat, so a
 // rep is one load).
 template <int KIND, int EPT>
-__global__ void __launch_bounds__(kThreads) k_scan(ScanArgs a) {
+__global__ void __launch_bounds__(kScanThreads, EPT == 16 ? 2 : 4) k_scan(ScanArgs a) {
   __shared__ int sidx[kSegCap + 1];
   __shared__ ReserveSmem sm;
   DevState* st = a.st;
@@ -245,23 +246,12 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanArgs a) {
   if (scan_ept(st->split) != EPT) return;  // only the variant the split selects runs
   const int thr = st->threshold;
   const int n = a.nodes, m = a.edges;
-  constexpr int kTile = kThreads * EPT;
+  constexpr int kTile = kScanThreads * EPT;
   constexpr int kStep = EPT / 4;  // first_v entries per tile
   const long long e0 = (long long)blockIdx.x * kTile;
   if (e0 >= m) return;
-  const int tb = blockIdx.x * kStep;
-  const int v_lo = __ldg(a.first_v + tb);
-  const int v_hi = __ldg(a.first_v + min(tb + kStep, a.tiles));
-  const int span = v_hi - v_lo + 1;  // vertices whose rows may hold this tile's entries
-  const bool seg = span <= kSegCap;
-  if (seg)
-    for (int i = threadIdx.x; i <= span; i += blockDim.x) sidx[i] = __ldg(a.nindex + v_lo + i);
-  __syncthreads();
-  auto row_start = [&](int i) -> int {  // nindex[v_lo + i]
-    return seg ? sidx[i] : __ldg(a.nindex + v_lo + i);
-  };
-
   const long long j0 = e0 + (long long)threadIdx.x * EPT;
+  // The tile's CSR loads go out first; the vertex lookup below overlaps them.
   int nb[EPT], w[EPT];
   if (j0 + EPT <= m && a.vec_ok) {
 #pragma unroll
@@ -279,6 +269,17 @@ __global__ void __launch_bounds__(kThreads) k_scan(ScanArgs a) {
       w[q] = in ? __ldg(a.eweight + j0 + q) : 0;
     }
   }
+  const int tb = blockIdx.x * kStep;
+  const int v_lo = __ldg(a.first_v + tb);
+  const int v_hi = __ldg(a.first_v + min(tb + kStep, a.tiles));
+  const int span = v_hi - v_lo + 1;  // vertices whose rows may hold this tile's entries
+  const bool seg = span <= kSegCap;
+  if (seg)
+    for (int i = threadIdx.x; i <= span; i += blockDim.x) sidx[i] = __ldg(a.nindex + v_lo + i);
+  __syncthreads();
+  auto row_start = [&](int i) -> int {  // nindex[v_lo + i]
+    return seg ? sidx[i] : __ldg(a.nindex + v_lo + i);
+  };
   if (KIND == kLight && j0 < m) {  // inMST = 0 (the reference memsets it, :306)
     if (a.zero_vec && j0 + EPT <= m) {
       if (EPT == 4) *reinterpret_cast<unsigned*>(a.inMST + j0) = 0u;
@@ -387,24 +388,29 @@ __device__ __forceinline__ unsigned pair_slot(u64 pk) {
   return (unsigned)((pk * 0x9E3779B97F4A7C15ull) >> (64 - kPairLog));
 }
 
-// Parallel-edge elimination in the contracted graph. Entries of one tile
-// that join the same two trees are parallel edges of the contracted graph;
-// only the one with the smallest (weight, j) key can be a forest edge (any
-// forest through a heavier one is heavier than the same forest through the
-// lightest), so the others are dropped for good. Warp groups with equal rep
-// pairs reduce first; group minima meet in a per-tile shared table. keep[k]
-// is narrowed to the survivors. Every thread of the CTA must call this.
+// Parallel-edge elimination in the contracted graph, fused with the tile's
+// worklist reservation. Entries of one tile that join the same two trees are
+// parallel edges of the contracted graph; only the one with the smallest
+// (weight, j) key can be a forest edge (any forest through a heavier one is
+// heavier than the same forest through the lightest), so the others are
+// dropped for good. Warp groups with equal rep pairs reduce first; group
+// minima meet in a per-tile shared table. keep[k] is narrowed to the
+// survivors, and *pos receives the first output slot of this thread's
+// survivors (one global atomic per CTA tile). Three CTA barriers in all.
+// Every thread of the CTA must call this.
 template <int E>
-__device__ __forceinline__ void drop_parallel(const int4 (&e)[E], bool (&keep)[E], RoundSmem& s) {
-  const int lane = threadIdx.x & 31;
+__device__ __forceinline__ void drop_parallel_reserve(const int4 (&e)[E], bool (&keep)[E],
+                                                      unsigned* ctr, RoundSmem& s, unsigned* pos) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   u64 pk[E], gmin[E];
 #pragma unroll
   for (int k = 0; k < E; k++) {
     const unsigned lo = (unsigned)min(e[k].x, e[k].y), hi = (unsigned)max(e[k].x, e[k].y);
     pk[k] = keep[k] ? (((u64)lo << 32) | hi) : (0xFFFFFFFF00000000ull | (threadIdx.x * E + k));
     const u64 key = edge_key(e[k].z, e[k].w);
-    const unsigned g = __match_any_sync(0xffffffffu, pk[k]);
     gmin[k] = key;
+#ifndef ECL_NO_DEDUP
+    const unsigned g = __match_any_sync(0xffffffffu, pk[k]);
     if (!keep[k]) continue;
     if (g & (g - 1)) {
       const unsigned khi = (unsigned)(key >> 32);
@@ -421,21 +427,48 @@ __device__ __forceinline__ void drop_parallel(const int4 (&e)[E], bool (&keep)[E
       }
       if (t == pk[k] && ((volatile u64*)s.pair_min)[slot] > gmin[k]) atomicMin(&s.pair_min[slot], gmin[k]);
     }
+#endif
   }
-  __syncthreads();
+  __syncthreads();  // S1: the tile's pair table is complete
+  unsigned cnt = 0;
 #pragma unroll
   for (int k = 0; k < E; k++) {
-    if (!keep[k]) continue;
-    const unsigned slot = pair_slot(pk[k]);
-    const u64 key = edge_key(e[k].z, e[k].w);
-    const u64 best = s.pair_tag[slot] == pk[k] ? s.pair_min[slot] : gmin[k];
-    keep[k] = key == best;
+#ifndef ECL_NO_DEDUP
+    if (keep[k]) {
+      const unsigned slot = pair_slot(pk[k]);
+      const u64 key = edge_key(e[k].z, e[k].w);
+      const u64 best = s.pair_tag[slot] == pk[k] ? s.pair_min[slot] : gmin[k];
+      keep[k] = key == best;
+    }
+#endif
+    cnt += keep[k];
   }
-  __syncthreads();
+  unsigned incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) s.rs.warp_off[warp][0] = incl;
+  __syncthreads();  // S2: every check done, warp totals written
   for (int i = threadIdx.x; i < kPairSlots; i += blockDim.x) {
     s.pair_tag[i] = kNoPair;
     s.pair_min[i] = kNoEdge;
   }
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    const unsigned w0 = lane < nw ? s.rs.warp_off[lane][0] : 0u;
+    unsigned x0 = w0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xffffffffu, x0, o);
+      if (lane >= o) x0 += t;
+    }
+    if (lane < nw) s.rs.warp_off[lane][0] = x0 - w0;
+    if (lane == 31) s.rs.base[0] = x0 ? atomicAdd(ctr, x0) : 0u;
+  }
+  __syncthreads();  // S3: offsets and the tile's base are published
+  *pos = s.rs.base[0] + s.rs.warp_off[warp][0] + (incl - cnt);
 }
 
 // Roots of the 2*kEPT endpoints a thread holds, all walks advanced in lock
@@ -600,20 +633,14 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
     }
     multi_find<N>(v, vv, a.parent, s);
     bool keep[kEPT];
-    unsigned cnt = 0;
 #pragma unroll
     for (int k = 0; k < kEPT; k++) {
       keep[k] = in_range[k] && v[2 * k] != v[2 * k + 1];
       e[k].x = v[2 * k];
       e[k].y = v[2 * k + 1];
     }
-#ifndef ECL_NO_DEDUP
-    drop_parallel<kEPT>(e, keep, s);
-#endif
-#pragma unroll
-    for (int k = 0; k < kEPT; k++) cnt += keep[k];
-    unsigned pos, unused;
-    cta_reserve2(cnt, 0u, out_ctr, nullptr, s.rs, pos, unused);
+    unsigned pos;
+    drop_parallel_reserve<kEPT>(e, keep, out_ctr, s, &pos);
     u64 key[N];
     bool kv[N];
 #pragma unroll

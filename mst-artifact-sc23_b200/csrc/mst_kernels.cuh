@@ -147,12 +147,28 @@ __device__ __forceinline__ void cta_reserve2(unsigned c0, unsigned c1, unsigned*
   __syncthreads();
 }
 
-// Root of v. parent[] only ever points to smaller or equal ids, so the walk
-// ends. Path splitting (each visited node is re-pointed to its grandparent)
-// is applied on the way: it only shortcuts inside one tree, so concurrent
-// finds still reach the same root, and it bounds the cost of long hook chains
-// (a path graph with increasing weights hooks every vertex under its
-// predecessor in one round). Must not run concurrently with unions.
+// Union-find order. A root is hooked under a root of higher priority, where
+// the priority is a fixed bijective 32-bit mix of the vertex id (the
+// MurmurHash3 finalizer): parent pointers therefore always lead to strictly
+// higher priority, so every walk ends and no cycle can form, and because the
+// priorities are a random permutation of the ids, the chains built when many
+// components merge in one round stay short in expectation (hooking by id, as
+// the reference join does with max -> min at ECL_MST.cu:137-144, builds a
+// chain as long as any id-monotone path of merging components).
+__device__ __forceinline__ unsigned uf_prio(int v) {
+  unsigned h = (unsigned)v;
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+
+// Root of v. Path splitting (each visited node is re-pointed to its
+// grandparent) is applied on the way: it only shortcuts inside one tree, so
+// concurrent finds still reach the same root. Must not run concurrently with
+// unions.
 __device__ __forceinline__ int find_halve(int v, int* parent) {
   int p = __ldcg(parent + v);
   while (p != v) {
@@ -174,17 +190,20 @@ __device__ __forceinline__ int find_ro(int v, const int* parent) {
   return v;
 }
 
-// Union of the trees holding a and b by CAS-hooking the larger root under the
-// smaller id. A failed CAS returns the node's current parent, which is smaller,
-// so the larger id of the pair strictly decreases and the loop ends.
+// Union of the trees holding a and b (ECL_MST.cu:137-144): CAS-hook the
+// lower-priority node under the higher-priority one if it is still a root;
+// a failed CAS returns its current parent, which has higher priority, so the
+// lower priority of the pair strictly increases and the loop ends.
 __device__ __forceinline__ void cas_union(int a, int b, int* parent) {
-  while (true) {
-    const int hi = a > b ? a : b, lo = a > b ? b : a;
-    if (hi == lo) return;
-    const int old = atomicCAS(parent + hi, hi, lo);
-    if (old == hi) return;
-    a = lo;
-    b = old;
+  while (a != b) {
+    if (uf_prio(a) > uf_prio(b)) {
+      const int t = a;
+      a = b;
+      b = t;
+    }
+    const int old = atomicCAS(parent + a, a, b);
+    if (old == a) return;
+    a = old;
   }
 }
 
