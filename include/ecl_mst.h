@@ -133,15 +133,21 @@ typedef struct mst_opts {
   int32_t threshold;      /* ECL_THRESH_EXPLICIT: edges with w <= threshold    */
                           /* form the first (light) phase                      */
   float quantile;         /* ECL_THRESH_QUANTILE, in [0,1]; >= 1 disables      */
-  int32_t degree_split;   /* rows with degree >= split are scanned by warps in */
-                          /* 128-entry chunks, shorter rows by one thread;     */
-                          /* 0 = default (32)                                  */
+  int32_t degree_split;   /* thread/cooperative split of the CSR scans: each   */
+                          /* thread takes E consecutive entries, E = 4 for     */
+                          /* split <= 4, 8 for split <= 8, else 16; rows       */
+                          /* shorter than E stay in one thread, longer rows    */
+                          /* are spread over threads/warps; 0 = default (8)    */
   int32_t block_size;     /* threads per CTA of the round kernel, 0 = default  */
   int32_t ctas_per_sm;    /* 0 = as many as fit                                */
   int32_t small_tail;     /* worklist size at which one CTA finishes the      */
                           /* rounds alone; 0 = default, < 0 = never            */
   int32_t flags;          /* ECL_FLAG_*                                        */
-  int32_t reserved[8];
+  int32_t batch_small_edges; /* batched mode: graphs with at most this many   */
+                          /* CSR entries (and fitting the per-CTA scratch) are */
+                          /* solved one per CTA by the persistent kernel;      */
+                          /* 0 = the context's per-CTA capacity                */
+  int32_t reserved[7];
 } mst_opts;
 
 /* Fill *opts with the defaults (heuristic threshold, reference semantics). */
@@ -217,6 +223,60 @@ int ecl_mst_run_device(ecl_mst_ctx* ctx, const ecl_graph* d_graph,
  *     (other threads, other streams) race and give wrong results. */
 int ecl_mst_run_device_noalloc(const ecl_graph* d_graph, uint8_t* d_inMST,
                                const mst_opts* opts, void* stream);
+
+/* ------------------------------------------------------------- batched mode */
+/* Many independent graphs in one call. Graph g has nodes[g] vertices and
+ * edges[g] CSR entries; its nindex (nodes[g] + 1 local offsets) starts at
+ * nindex[nindex_off[g]], its local neighbour ids and weights at
+ * nlist[edge_off[g]] / eweight[edge_off[g]], and its inMST flags are written
+ * at inMST[edge_off[g]]. nodes/edges/nindex_off/edge_off are HOST arrays,
+ * nindex/nlist/eweight DEVICE arrays. Segments may be padded (offsets that
+ * are multiples of 4 entries keep 128-bit loads aligned). Each graph gets the
+ * reference treatment (its own threshold per opts, its own rounds), with
+ * results identical to solving it alone. */
+typedef struct ecl_batch {
+  int32_t num_graphs;
+  const int32_t* nodes;
+  const int32_t* edges;
+  const int64_t* nindex_off;
+  const int64_t* edge_off;
+  int32_t* nindex;
+  int32_t* nlist;
+  int32_t* eweight;
+} ecl_batch;
+
+typedef struct ecl_batch_stats {
+  int32_t graphs_small;  /* solved one per CTA in the persistent launch */
+  int32_t graphs_large;  /* solved by the grid-wide engine                */
+  int32_t status;        /* device error word                             */
+  int32_t graph_replay;  /* 1 if the large graphs ran from a CUDA graph     */
+  int64_t edges_total;
+  float ms_total, ms_small, ms_large;
+} ecl_batch_stats;
+
+typedef struct ecl_batch_ctx ecl_batch_ctx;
+
+/* Workspace for batches of up to max_graphs graphs, none larger than
+ * (max_graph_nodes, max_graph_edges). small_cap sizes the per-CTA scratch of
+ * the persistent kernel (vertices and entries of the largest graph it may
+ * take; 0 = 2^19). */
+int ecl_batch_ctx_create(int device, int32_t max_graphs, int64_t max_graph_nodes,
+                         int64_t max_graph_edges, int32_t small_cap,
+                         ecl_batch_ctx** out);
+void ecl_batch_ctx_destroy(ecl_batch_ctx* ctx);
+
+/* Solve every graph of the batch (device-resident, on `stream` or the
+ * context's stream). Returns after completion when stats != NULL. */
+int ecl_mst_run_batch_device(ecl_batch_ctx* ctx, const ecl_batch* batch,
+                             uint8_t* d_inMST, const mst_opts* opts, void* stream,
+                             ecl_batch_stats* stats);
+
+/* Autotuner: times candidate schedules (per-CTA cutoff, scan entries per
+ * thread, single-CTA tail size) on the batch and writes the fastest into
+ * *best (a copy of *base with those fields set). The answer is the same for
+ * every candidate; only the time differs. */
+int ecl_batch_autotune(ecl_batch_ctx* ctx, const ecl_batch* batch, uint8_t* d_inMST,
+                       const mst_opts* base, mst_opts* best, float* best_ms);
 
 /* Wait for the context's stream and report a device-side error if any. */
 int ecl_mst_ctx_sync(ecl_mst_ctx* ctx);

@@ -13,6 +13,8 @@
 #include "ecl_mst.h"
 #include "internal.h"
 #include "mst_device.cuh"
+#include "batch_device.cuh"
+#include <vector>
 
 using namespace ecl;
 
@@ -583,4 +585,326 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   ECL_CUDA_TRY(cudaMemcpyAsync(&err, &dst->error, sizeof(err), cudaMemcpyDeviceToHost, s));
   ECL_CUDA_TRY(cudaStreamSynchronize(s));
   return device_error_status(err);
+}
+
+// ============================================================== batched mode
+namespace {
+
+__global__ void k_or_error(const DevState* src, DevState* dst) {
+  const unsigned e = ld_volatile(&src->error);
+  if (e) atomicOr(&dst->error, e);
+}
+
+constexpr int kBatchDefaultCap = 1 << 19;
+
+}  // namespace
+
+struct ecl_batch_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+  int max_graphs = 0;
+  int64_t max_nodes = 0, max_edges = 0;
+  int cap = 0;        // per-CTA scratch: vertices and CSR entries
+  int small_grid = 0; // CTAs of the persistent kernel
+  int* parent_pool = nullptr;
+  u64* minv_pool = nullptr;
+  int4* wl_pool = nullptr;
+  long long* d_node_off = nullptr;
+  long long* d_edge_off = nullptr;
+  int* d_small = nullptr;
+  unsigned* d_queue = nullptr;
+  DevState* st = nullptr;
+  ecl_mst_ctx* big = nullptr;  // grid-wide engine for graphs beyond the cutoff
+  cudaEvent_t ev[3] = {};
+  // the large-graph launch sequence captured as a CUDA graph, keyed by the batch
+  cudaGraphExec_t exec = nullptr;
+  std::vector<long long> exec_key;
+};
+
+extern "C" void ecl_batch_ctx_destroy(ecl_batch_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->exec) cudaGraphExecDestroy(c->exec);
+  cudaFree(c->parent_pool);
+  cudaFree(c->minv_pool);
+  cudaFree(c->wl_pool);
+  cudaFree(c->d_node_off);
+  cudaFree(c->d_edge_off);
+  cudaFree(c->d_small);
+  cudaFree(c->d_queue);
+  cudaFree(c->st);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  ecl_mst_ctx_destroy(c->big);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+extern "C" int ecl_batch_ctx_create(int device, int32_t max_graphs, int64_t max_graph_nodes,
+                                    int64_t max_graph_edges, int32_t small_cap, ecl_batch_ctx** out) {
+  if (!out || max_graphs < 1 || max_graph_nodes < 1 || max_graph_edges < 0 || small_cap < 0)
+    return ECL_ERR_INVALID_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return ECL_ERR_NO_DEVICE;
+  if (device < 0 || device >= ndev) return ECL_ERR_INVALID_ARG;
+  ECL_CUDA_TRY(cudaSetDevice(device));
+  ecl_batch_ctx* c = new (std::nothrow) ecl_batch_ctx();
+  if (!c) return ECL_ERR_ALLOC;
+  c->device = device;
+  c->max_graphs = max_graphs;
+  c->max_nodes = max_graph_nodes;
+  c->max_edges = max_graph_edges;
+  c->cap = small_cap > 0 ? small_cap : kBatchDefaultCap;
+  int st;
+  auto fail = [&](int s) {
+    ecl_batch_ctx_destroy(c);
+    return s;
+  };
+  if ((st = cuda_status(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device))))
+    return fail(st);
+  if ((st = cuda_status(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)))) return fail(st);
+  int per_sm = 0;
+  if ((st = cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_batch_small,
+                                                                      kThreads, 0))))
+    return fail(st);
+  c->small_grid = std::max(1, per_sm) * c->sm_count;
+  const size_t ctas = (size_t)c->small_grid, cap = (size_t)c->cap;
+  if ((st = cuda_status(cudaMalloc(&c->parent_pool, ctas * cap * sizeof(int))))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->minv_pool, ctas * 2 * cap * sizeof(u64))))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->wl_pool, ctas * 2 * cap * sizeof(int4))))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->d_node_off, 2 * (size_t)max_graphs * sizeof(long long))))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->d_edge_off, 2 * (size_t)max_graphs * sizeof(long long))))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->d_small, (size_t)max_graphs * sizeof(int))))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->d_queue, sizeof(unsigned))))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->st, sizeof(DevState))))) return fail(st);
+  for (auto& e : c->ev)
+    if ((st = cuda_status(cudaEventCreate(&e)))) return fail(st);
+  if (max_graph_edges > c->cap || max_graph_nodes > c->cap) {
+    if ((st = ecl_mst_ctx_create(device, max_graph_nodes, std::max<int64_t>(max_graph_edges, 1), &c->big)))
+      return fail(st);
+  }
+  *out = c;
+  return ECL_OK;
+}
+
+namespace {
+
+// Per-graph descriptors for the persistent kernel use the "nodes / edges"
+// form: node_off[g] = nindex_off[g] - g keeps nindex at node_off[g] + g, and
+// edge_off[g + 1] - edge_off[g] must give edges[g], so the kernel gets its own
+// compact offset arrays built here (one entry per small graph, in queue order).
+int batch_enqueue(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST, const mst_opts* o,
+                  cudaStream_t s, bool timed, ecl_batch_stats* stats) {
+  const int G = b->num_graphs;
+  const int cutoff = std::min(o->batch_small_edges > 0 ? o->batch_small_edges : c->cap, c->cap);
+  std::vector<int> small, large;
+  int64_t edges_total = 0;
+  for (int g = 0; g < G; g++) {
+    const int n = b->nodes[g], m = b->edges[g];
+    if (n < 1 || m < 0) return ECL_ERR_INVALID_ARG;
+    if (n > c->max_nodes || m > c->max_edges) return ECL_ERR_TOO_LARGE;
+    edges_total += m;
+    if (m <= cutoff && n <= c->cap) small.push_back(g);
+    else large.push_back(g);
+  }
+  if (!large.empty() && !c->big) return ECL_ERR_TOO_LARGE;
+  // largest first: the persistent kernel's tail then consists of small graphs
+  std::sort(small.begin(), small.end(), [&](int x, int y) { return b->edges[x] > b->edges[y]; });
+  // compact descriptors: small graph i -> (node_off, edge_off) pairs at i, i + 1
+  const int S = (int)small.size();
+  std::vector<long long> noff(2 * (size_t)S), eoff(2 * (size_t)S);
+  std::vector<int> ids(S);
+  for (int i = 0; i < S; i++) {
+    const int g = small[i];
+    noff[2 * i] = b->nindex_off[g] - 2 * (long long)i;     // + id (= 2i) gives nindex_off
+    noff[2 * i + 1] = noff[2 * i] + b->nodes[g];
+    eoff[2 * i] = b->edge_off[g];
+    eoff[2 * i + 1] = b->edge_off[g] + b->edges[g];
+    ids[i] = 2 * i;
+  }
+  ECL_CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevState), s));
+  ECL_CUDA_TRY(cudaMemsetAsync(c->d_queue, 0, sizeof(unsigned), s));
+  if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  if (S > 0) {
+    ECL_CUDA_TRY(cudaMemcpyAsync(c->d_node_off, noff.data(), noff.size() * sizeof(long long),
+                                 cudaMemcpyHostToDevice, s));
+    ECL_CUDA_TRY(cudaMemcpyAsync(c->d_edge_off, eoff.data(), eoff.size() * sizeof(long long),
+                                 cudaMemcpyHostToDevice, s));
+    ECL_CUDA_TRY(cudaMemcpyAsync(c->d_small, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    BatchArgs ba;
+    ba.num_small = S;
+    ba.small_list = c->d_small;
+    ba.node_off = c->d_node_off;
+    ba.edge_off = c->d_edge_off;
+    ba.nindex = b->nindex;
+    ba.nlist = b->nlist;
+    ba.eweight = b->eweight;
+    ba.inMST = d_inMST;
+    ba.parent_pool = c->parent_pool;
+    ba.minv_pool = c->minv_pool;
+    ba.wl_pool = c->wl_pool;
+    ba.cap_n = c->cap;
+    ba.cap_m = c->cap;
+    ba.queue = c->d_queue;
+    ba.st = c->st;
+    ba.mode = o->threshold_mode == ECL_THRESH_LEARNED ? ECL_THRESH_HEURISTIC : o->threshold_mode;
+    ba.explicit_thr = o->threshold;
+    ba.quantile = o->quantile;
+    ba.count_atomics = (o->flags & ECL_FLAG_STATS) ? 1 : 0;
+    const int grid = std::min(c->small_grid, S);
+    k_batch_small<<<grid, kThreads, 0, s>>>(ba);
+    ECL_CUDA_TRY(cudaGetLastError());
+  }
+  if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  bool replayed = false;
+  if (!large.empty()) {
+    // The large graphs' launch sequence (per graph: control-block reset and
+    // six kernels, no host round trip) is captured once per batch layout as a
+    // CUDA graph and replayed; if capture is unavailable it is enqueued.
+    std::vector<long long> key;
+    key.push_back((long long)(uintptr_t)b->nindex);
+    key.push_back((long long)(uintptr_t)b->nlist);
+    key.push_back((long long)(uintptr_t)b->eweight);
+    key.push_back((long long)(uintptr_t)d_inMST);
+    key.push_back(o->threshold_mode);
+    key.push_back(o->threshold);
+    key.push_back((long long)(o->quantile * 1e6f));
+    key.push_back(o->degree_split);
+    key.push_back(o->small_tail);
+    key.push_back(o->flags);
+    for (int g : large) {
+      key.push_back(g);
+      key.push_back(b->nindex_off[g]);
+      key.push_back(b->edge_off[g]);
+      key.push_back(b->nodes[g]);
+      key.push_back(b->edges[g]);
+    }
+    mst_opts lo = *o;
+    if (lo.threshold_mode == ECL_THRESH_LEARNED) lo.threshold_mode = ECL_THRESH_HEURISTIC;
+    auto enqueue_large = [&](cudaStream_t q) -> int {
+      for (int g : large) {
+        ecl_graph dg = {b->nodes[g], b->edges[g], b->nindex + b->nindex_off[g], b->nlist + b->edge_off[g],
+                        b->eweight + b->edge_off[g]};
+        ECL_CUDA_TRY(cudaMemsetAsync(c->big->st, 0, sizeof(DevState), q));
+        int r = enqueue_solve(c->big, &dg, d_inMST + b->edge_off[g], &lo, q, false);
+        if (r) return r;
+        k_or_error<<<1, 1, 0, q>>>(c->big->st, c->st);
+        ECL_CUDA_TRY(cudaGetLastError());
+      }
+      return ECL_OK;
+    };
+    if (c->exec && c->exec_key == key) {
+      ECL_CUDA_TRY(cudaGraphLaunch(c->exec, s));
+      replayed = true;
+    } else {
+      if (c->exec) {
+        cudaGraphExecDestroy(c->exec);
+        c->exec = nullptr;
+      }
+      cudaGraph_t graph = nullptr;
+      bool captured = false;
+      if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const int r = enqueue_large(s);
+        const cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (r == ECL_OK && e == cudaSuccess && graph &&
+            cudaGraphInstantiate(&c->exec, graph, 0) == cudaSuccess) {
+          captured = true;
+          c->exec_key = key;
+        }
+        if (graph) cudaGraphDestroy(graph);
+      }
+      cudaGetLastError();  // clear a failed capture's error state
+      if (captured) {
+        ECL_CUDA_TRY(cudaGraphLaunch(c->exec, s));
+        replayed = true;
+      } else {
+        c->exec = nullptr;
+        int r = enqueue_large(s);
+        if (r) return r;
+      }
+    }
+  }
+  if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->graphs_small = S;
+    stats->graphs_large = (int)large.size();
+    stats->graph_replay = replayed ? 1 : 0;
+    stats->edges_total = edges_total;
+  }
+  return ECL_OK;
+}
+
+int batch_finish(ecl_batch_ctx* c, cudaStream_t s, ecl_batch_stats* stats) {
+  ECL_CUDA_TRY(cudaStreamSynchronize(s));
+  unsigned err = 0;
+  ECL_CUDA_TRY(cudaMemcpy(&err, &c->st->error, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (stats) {
+    stats->status = (int32_t)err;
+    cudaEventElapsedTime(&stats->ms_small, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&stats->ms_large, c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&stats->ms_total, c->ev[0], c->ev[2]);
+  }
+  return device_error_status(err);
+}
+
+}  // namespace
+
+extern "C" int ecl_mst_run_batch_device(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST,
+                                        const mst_opts* opts, void* stream, ecl_batch_stats* stats) {
+  if (!c || !b || !d_inMST || b->num_graphs < 0 || !b->nodes || !b->edges || !b->nindex_off ||
+      !b->edge_off || !b->nindex)
+    return ECL_ERR_INVALID_ARG;
+  if (b->num_graphs > c->max_graphs) return ECL_ERR_TOO_LARGE;
+  mst_opts o;
+  if (opts) o = *opts;
+  else ecl_default_opts(&o);
+  int st = check_opts(&o);
+  if (st) return st;
+  ECL_CUDA_TRY(cudaSetDevice(c->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  if ((st = batch_enqueue(c, b, d_inMST, &o, s, stats != nullptr, stats))) return st;
+  if (stats) return batch_finish(c, s, stats);
+  return ECL_OK;
+}
+
+extern "C" int ecl_batch_autotune(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST,
+                                  const mst_opts* base, mst_opts* best, float* best_ms) {
+  if (!c || !b || !best) return ECL_ERR_INVALID_ARG;
+  mst_opts o0;
+  if (base) o0 = *base;
+  else ecl_default_opts(&o0);
+  float best_t = 1e30f;
+  mst_opts best_o = o0;
+  const int cutoffs[] = {c->cap / 8, c->cap / 2, c->cap};
+  const int splits[] = {8, 16};
+  const int tails[] = {4096, 16384};
+  for (int cut : cutoffs) {
+    if (cut < 1) continue;
+    for (int sp : splits) {
+      for (int tl : tails) {
+        mst_opts o = o0;
+        o.batch_small_edges = cut;
+        o.degree_split = sp;
+        o.small_tail = tl;
+        float t = 0.f;
+        for (int rep = 0; rep < 3; rep++) {
+          ecl_batch_stats bs;
+          int st = ecl_mst_run_batch_device(c, b, d_inMST, &o, nullptr, &bs);
+          if (st) return st;
+          if (rep > 0) t += bs.ms_total;  // first run warms up (and captures)
+        }
+        if (t < best_t) {
+          best_t = t;
+          best_o = o;
+        }
+      }
+    }
+  }
+  *best = best_o;
+  if (best_ms) *best_ms = best_t / 2;
+  return ECL_OK;
 }

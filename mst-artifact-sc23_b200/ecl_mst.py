@@ -46,7 +46,8 @@ class EclGraphC(ctypes.Structure):
 class MstOpts(ctypes.Structure):
     _fields_ = [("threshold_mode", c_int32), ("threshold", c_int32), ("quantile", c_float),
                 ("degree_split", c_int32), ("block_size", c_int32), ("ctas_per_sm", c_int32),
-                ("small_tail", c_int32), ("flags", c_int32), ("reserved", c_int32 * 8)]
+                ("small_tail", c_int32), ("flags", c_int32), ("batch_small_edges", c_int32),
+                ("reserved", c_int32 * 7)]
 
 
 class MstStats(ctypes.Structure):
@@ -69,6 +70,20 @@ class MstStats(ctypes.Structure):
             "us_scan": [list(self.us_scan[p]) for p in range(2)],
             "us_round": [[list(self.us_round[p][r]) for r in range(max(self.rounds[p], 0))] for p in range(2)],
         }
+
+
+class EclBatchC(ctypes.Structure):
+    _fields_ = [("num_graphs", c_int32), ("nodes", c_void_p), ("edges", c_void_p), ("nindex_off", c_void_p),
+                ("edge_off", c_void_p), ("nindex", c_void_p), ("nlist", c_void_p), ("eweight", c_void_p)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("graphs_small", c_int32), ("graphs_large", c_int32), ("status", c_int32),
+                ("graph_replay", c_int32), ("edges_total", c_int64), ("ms_total", c_float),
+                ("ms_small", c_float), ("ms_large", c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 _lib = None
@@ -107,6 +122,12 @@ def load():
         "ecl_mst_ctx_stream": (c_void_p, [c_void_p]),
         "ecl_host_alloc_pinned": (c_int, [ctypes.c_size_t, POINTER(c_void_p)]),
         "ecl_host_free_pinned": (None, [c_void_p]),
+        "ecl_batch_ctx_create": (c_int, [c_int, c_int32, c_int64, c_int64, c_int32, POINTER(c_void_p)]),
+        "ecl_batch_ctx_destroy": (None, [c_void_p]),
+        "ecl_mst_run_batch_device": (c_int, [c_void_p, POINTER(EclBatchC), c_void_p, POINTER(MstOpts), c_void_p,
+                                             POINTER(BatchStats)]),
+        "ecl_batch_autotune": (c_int, [c_void_p, POINTER(EclBatchC), c_void_p, POINTER(MstOpts), POINTER(MstOpts),
+                                       POINTER(c_float)]),
         "ecl_verify": (c_int, [G, c_void_p, c_void_p, POINTER(c_int64), POINTER(c_uint64), POINTER(c_uint64)]),
         "ecl_forest_weight": (c_uint64, [G, c_void_p]),
     }
@@ -308,3 +329,80 @@ class Context:
 
     def sync(self):
         _check(self._lib.ecl_mst_ctx_sync(self.handle), "ctx_sync")
+
+
+class Batch:
+    """Host-side packing of many graphs into one batch layout (ecl_batch).
+
+    Segments start at multiples of `align` entries so 128-bit loads stay
+    aligned; nindex of graph g sits at nindex_off[g], its entries at edge_off[g].
+    """
+
+    def __init__(self, graphs, align=4):
+        self.num_graphs = len(graphs)
+        self.nodes = np.array([g.nodes for g in graphs], np.int32)
+        self.edges = np.array([g.edges for g in graphs], np.int32)
+        noff, eoff = [], []
+        no = eo = 0
+        for g in graphs:
+            noff.append(no)
+            eoff.append(eo)
+            no += -(-(g.nodes + 1) // align) * align
+            eo += -(-max(g.edges, 1) // align) * align
+        self.nindex_off = np.array(noff, np.int64)
+        self.edge_off = np.array(eoff, np.int64)
+        self.total_nindex, self.total_edges = no, eo
+        self.nindex = np.zeros(no, np.int32)
+        self.nlist = np.zeros(eo, np.int32)
+        self.eweight = np.zeros(eo, np.int32)
+        for g, a, b in zip(graphs, noff, eoff):
+            self.nindex[a:a + g.nodes + 1] = g.nindex
+            self.nlist[b:b + g.edges] = g.nlist
+            self.eweight[b:b + g.edges] = g.eweight
+
+    def struct(self, d_nindex, d_nlist, d_eweight):
+        return EclBatchC(self.num_graphs, _ptr(self.nodes), _ptr(self.edges), _ptr(self.nindex_off),
+                         _ptr(self.edge_off), d_nindex, d_nlist, d_eweight)
+
+    def slice(self, inmst, g):
+        a = int(self.edge_off[g])
+        return inmst[a:a + int(self.edges[g])]
+
+
+class BatchContext:
+    """Workspace of the batched engine (ecl_batch_ctx)."""
+
+    def __init__(self, max_graphs, max_graph_nodes, max_graph_edges, small_cap=0, device=0):
+        self._lib = load()
+        h = c_void_p()
+        _check(self._lib.ecl_batch_ctx_create(device, max_graphs, max_graph_nodes, max_graph_edges, small_cap,
+                                              ctypes.byref(h)), "batch_ctx_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            self._lib.ecl_batch_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, batch, d_nindex, d_nlist, d_eweight, d_inMST, opts=None, stream=None):
+        bs = batch.struct(d_nindex, d_nlist, d_eweight)
+        st = BatchStats()
+        _check(self._lib.ecl_mst_run_batch_device(self.handle, ctypes.byref(bs), d_inMST,
+                                                  None if opts is None else ctypes.byref(opts), stream,
+                                                  ctypes.byref(st)), "run_batch")
+        return st.as_dict()
+
+    def autotune(self, batch, d_nindex, d_nlist, d_eweight, d_inMST, base=None):
+        bs = batch.struct(d_nindex, d_nlist, d_eweight)
+        best = MstOpts()
+        ms = c_float()
+        _check(self._lib.ecl_batch_autotune(self.handle, ctypes.byref(bs), d_inMST,
+                                            None if base is None else ctypes.byref(base), ctypes.byref(best),
+                                            ctypes.byref(ms)), "batch_autotune")
+        return best, ms.value

@@ -1,0 +1,89 @@
+"""Batched mode: many graphs of uneven sizes in one call, each bit-identical
+to solving it alone (oracle), through the persistent one-CTA-per-graph launch
+and the grid-wide engine (captured as a CUDA graph) for graphs beyond the
+per-CTA cutoff."""
+import numpy as np
+import pytest
+
+import ecl_mst as E
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixed_graphs(seed0, count):
+    rng = np.random.default_rng(seed0)
+    gs = []
+    for i in range(count):
+        fam = i % 4
+        n = int(np.exp(rng.uniform(np.log(50), np.log(60000))))
+        s = seed0 + i
+        if fam == 0:
+            r = max(2, int(np.sqrt(n)))
+            gs.append(E.gen_grid(r, max(1, n // r), s, 1 << 20))
+        elif fam == 1:
+            gs.append(E.gen_er(n, 8, s, 1 << 20))
+        elif fam == 2:
+            gs.append(E.gen_rmat(max(6, int(np.log2(n))), 8, 0.57, 0.19, 0.19, s, 1 << 20))
+        else:
+            gs.append(E.gen_rgg2d(n, 3, s, 1 << 20))
+    gs.append(E.Graph(np.array([0, 0], np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32)))  # 1 vertex
+    return gs
+
+
+def _run(graphs, small_cap, opts_list):
+    import torch
+    b = E.Batch(graphs)
+    dev = torch.device("cuda:0")
+    ni = torch.from_numpy(b.nindex).to(dev)
+    nl = torch.from_numpy(b.nlist).to(dev)
+    ew = torch.from_numpy(b.eweight).to(dev)
+    out = torch.zeros(b.total_edges, dtype=torch.uint8, device=dev)
+    bc = E.BatchContext(len(graphs), max(g.nodes for g in graphs), max(g.edges for g in graphs), small_cap)
+    wants = []
+    for g in graphs:
+        t, f = E.heuristic_threshold(g) if g.edges else (2**31 - 1, 0)
+        wants.append(O.oracle_mst(g.nindex, g.nlist, g.eweight, t, f)[0])
+    results = []
+    for o in opts_list:
+        for rep in range(2):  # second run replays the captured large-graph sequence
+            out.fill_(3)
+            st = bc.run(b, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(), opts=o)
+            got = out.cpu().numpy()
+            for gi, g in enumerate(graphs):
+                assert np.array_equal(b.slice(got, gi), wants[gi]), (gi, g.nodes, g.edges, rep)
+            results.append(st)
+    bc.close()
+    return results
+
+
+def test_batch_all_small():
+    sts = _run(_mixed_graphs(1000, 40), 1 << 19, [None])
+    assert sts[0]["graphs_large"] == 0 and sts[0]["status"] == 0
+
+
+def test_batch_mixed_small_and_large():
+    opts = [None, E.make_opts(mode=E.THRESH_QUANTILE, quantile=0.05, degree_split=16, small_tail=1024)]
+    sts = _run(_mixed_graphs(2000, 40), 1 << 12, opts)
+    assert all(s["graphs_large"] > 0 and s["graphs_small"] > 0 for s in sts)
+    assert sts[1]["graph_replay"] == 1
+
+
+def test_batch_autotune_keeps_the_answer():
+    import torch
+    graphs = _mixed_graphs(3000, 16)
+    b = E.Batch(graphs)
+    dev = torch.device("cuda:0")
+    ni = torch.from_numpy(b.nindex).to(dev)
+    nl = torch.from_numpy(b.nlist).to(dev)
+    ew = torch.from_numpy(b.eweight).to(dev)
+    out = torch.zeros(b.total_edges, dtype=torch.uint8, device=dev)
+    bc = E.BatchContext(len(graphs), max(g.nodes for g in graphs), max(g.edges for g in graphs), 1 << 13)
+    best, ms = bc.autotune(b, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr())
+    assert ms > 0 and best.batch_small_edges > 0
+    bc.run(b, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(), opts=best)
+    got = out.cpu().numpy()
+    for gi, g in enumerate(graphs):
+        t, f = E.heuristic_threshold(g) if g.edges else (2**31 - 1, 0)
+        assert np.array_equal(b.slice(got, gi), O.oracle_mst(g.nindex, g.nlist, g.eweight, t, f)[0])
+    bc.close()
