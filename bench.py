@@ -166,6 +166,67 @@ def scan_kernel_bytes(st, nodes, edges, entry_bytes=16):
     return b
 
 
+def batch_leg(args, E, torch, dev):
+    """Mixed-family batch (graphs seeded 1000, 1001, ...; sizes log-uniform in
+    [1e3, 2e6] vertices; grid / ER deg 8 / RMAT ef 8 / RGG2D deg 3; weights
+    U[1, 2^20]): the first `args.batch` graphs of the 4096-graph sequence, solved
+    in one batched call, against looping the plain ECL-MST over the same graphs."""
+    t0 = time.perf_counter()
+    graphs = E.gen_batch(args.batch)
+    gen_s = time.perf_counter() - t0
+    b = E.Batch(graphs)
+    total_m = int(b.edges.sum())
+    ni = torch.from_numpy(b.nindex).to(dev)
+    nl = torch.from_numpy(b.nlist).to(dev)
+    ew = torch.from_numpy(b.eweight).to(dev)
+    out = torch.zeros(b.total_edges, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    bc = E.BatchContext(len(graphs), int(b.nodes.max()), int(b.edges.max()), 1 << 19)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    best, tune_ms = bc.autotune(b, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr())
+    for _ in range(2):
+        bc.run(b, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(), opts=best, stream=stream)
+    ms = []
+    last = None
+    for _ in range(max(3, args.steps // 2)):
+        flush.zero_()
+        last = bc.run(b, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(), opts=best, stream=stream)
+        ms.append(last["ms_total"])
+    t = sum(ms) / len(ms)
+    got = out.cpu().numpy()
+    res = {"graphs": len(graphs), "edges": total_m, "ms": t, "graphs_per_s": len(graphs) / (t * 1e-3),
+           "gedges_per_s": total_m / (t * 1e-3) / 1e9, "graphs_small": last["graphs_small"],
+           "graphs_large": last["graphs_large"], "cuda_graph_replay": last["graph_replay"],
+           "autotuned": {"batch_small_edges": best.batch_small_edges, "degree_split": best.degree_split,
+                         "small_tail": best.small_tail},
+           "gen_s": round(gen_s, 1),
+           "sample": f"first {len(graphs)} graphs of the 4096-graph mixed batch (seeds 1000..{999 + len(graphs)})"}
+    plain_so = os.path.join(ROOT, "baseline", "_ref", "libecl_plain.so")
+    if os.path.exists(plain_so) and not args.no_plain:
+        import ctypes
+        lib = ctypes.CDLL(plain_so)
+        P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        tot = 0.0
+        same = True
+        for gi, g in enumerate(graphs):
+            if g.edges == 0:
+                continue
+            f, th = ctypes.c_int(), ctypes.c_int()
+            lib.plain_threshold(g.nodes, g.edges, P(g.eweight), ctypes.byref(f), ctypes.byref(th))
+            pout = np.zeros(g.edges, np.uint8)
+            s = ctypes.c_double()
+            lib.plain_gpu_mst(g.nodes, g.edges, P(g.nindex), P(g.nlist), P(g.eweight), f, th, P(pout),
+                              ctypes.byref(s))
+            tot += s.value
+            same &= bool(np.array_equal(pout, b.slice(got, gi)))
+        res["plain"] = {"ms": tot * 1e3, "graphs_per_s": len(graphs) / tot, "gedges_per_s": total_m / tot / 1e9,
+                        "inMST_identical": same,
+                        "what": "reference gpuMST rebuilt for sm_100a, looped over the graphs, sum of its own timed windows"}
+        res["vs_plain_graphs_per_s"] = res["graphs_per_s"] / res["plain"]["graphs_per_s"]
+    bc.close()
+    return res
+
+
 def reference_arm(args, E):
     """bench.py --impl reference: the reference's cpuMST on the host cores."""
     rank = int(os.environ.get("RANK", "0"))
@@ -210,6 +271,8 @@ def main():
     ap.add_argument("--split", type=int, default=0)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain ECL-MST comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--batch", type=int, default=256,
+                    help="graphs of the mixed batch to solve in batched mode (0 = skip)")
     ap.add_argument("--profile", action="store_true",
                     help="device solves only (no e2e, plain or CPU legs): the command profiled by ncu")
     args = ap.parse_args()
@@ -362,6 +425,10 @@ def main():
                  "runs": len(secs) - 1, "inMST_identical": bool(np.array_equal(pout[: g.edges], inmst)),
                  "what": "reference ECL_MST.cu gpuMST rebuilt for sm_100a, its own timed window, median"}
 
+    batch = None
+    if rank == 0 and args.batch > 0 and world == 1:
+        batch = batch_leg(args, E, torch, dev)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -392,6 +459,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "plain_ecl_mst": plain,
+            "batch": batch,
             "vs_plain": (value / plain["value"]) if plain else None,
             "forest_weight": fw,
             "clocks": clocks,

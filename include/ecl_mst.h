@@ -105,6 +105,13 @@ int ecl_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b,
 int ecl_gen_rgg2d(int32_t nodes, double avg_degree, uint64_t seed,
                   int32_t wmax, int threads, ecl_graph* out);
 
+/* Graph `index` of the mixed-family batch: seed seed0 + index, family uniform
+ * over {2D grid, Erdos-Renyi avg degree 8, RMAT (.57,.19,.19) edge factor 8,
+ * random geometric 2D avg degree 3}, vertex count log-uniform in
+ * [nmin, nmax]; *family receives 0..3 in that order. Single-threaded. */
+int ecl_gen_batch_graph(int32_t index, uint64_t seed0, int32_t nmin, int32_t nmax,
+                        int32_t wmax, ecl_graph* out, int32_t* family);
+
 /* ------------------------------------------------------------- threshold */
 typedef enum ecl_threshold_mode {
   ECL_THRESH_HEURISTIC = 0, /* the reference rule (ECL_MST.cu:408,432-444)      */

@@ -271,3 +271,35 @@ extern "C" int ecl_gen_rgg2d(int32_t nodes, double avg_degree, uint64_t seed, in
   for (auto& p : part) pairs.insert(pairs.end(), p.begin(), p.end());
   return build_csr(nodes, pairs, seed, wmax, threads, out);
 }
+
+// Graph `index` of the mixed batch: seed = seed0 + index; the family is
+// uniform over {grid, Erdos-Renyi (avg degree 8), RMAT (0.57, 0.19, 0.19,
+// edge factor 8), random geometric 2D (avg degree 3)} and the vertex count
+// log-uniform in [nmin, nmax] (RMAT rounds it to a power of two, the grid to
+// rows x cols with rows = floor(sqrt(n))). Single-threaded, so many graphs
+// can be generated in parallel.
+extern "C" int ecl_gen_batch_graph(int32_t index, uint64_t seed0, int32_t nmin, int32_t nmax,
+                                   int32_t wmax, ecl_graph* out, int32_t* family) {
+  if (!out || nmin < 1 || nmax < nmin || index < 0) return ECL_ERR_INVALID_ARG;
+  const uint64_t seed = seed0 + (uint64_t)index;
+  const uint64_t r0 = ecl_rng(seed, 5, 0), r1 = ecl_rng(seed, 5, 1);
+  const int fam = (int)(r0 % 4);
+  const double u = (double)(r1 >> 11) * (1.0 / 9007199254740992.0);
+  const double ln = std::log((double)nmin) + u * (std::log((double)nmax) - std::log((double)nmin));
+  const int32_t n = (int32_t)std::max<double>(nmin, std::min<double>(nmax, std::llround(std::exp(ln))));
+  if (family) *family = fam;
+  switch (fam) {
+    case 0: {
+      const int32_t rows = std::max<int32_t>(1, (int32_t)std::sqrt((double)n));
+      return ecl_gen_grid(rows, std::max<int32_t>(1, n / rows), seed, wmax, 1, out);
+    }
+    case 1:
+      return ecl_gen_er(n, 8.0, seed, wmax, 1, out);
+    case 2: {
+      const int32_t scale = std::max<int32_t>(1, (int32_t)std::lround(std::log2((double)n)));
+      return ecl_gen_rmat(scale, 8, 0.57, 0.19, 0.19, seed, wmax, 1, out);
+    }
+    default:
+      return ecl_gen_rgg2d(n, 3.0, seed, wmax, 1, out);
+  }
+}

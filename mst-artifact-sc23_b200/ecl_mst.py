@@ -110,6 +110,7 @@ def load():
         "ecl_gen_er": (c_int, [c_int32, c_double, c_uint64, c_int32, c_int, G]),
         "ecl_gen_rmat": (c_int, [c_int32, c_int32, c_double, c_double, c_double, c_uint64, c_int32, c_int, G]),
         "ecl_gen_rgg2d": (c_int, [c_int32, c_double, c_uint64, c_int32, c_int, G]),
+        "ecl_gen_batch_graph": (c_int, [c_int32, c_uint64, c_int32, c_int32, c_int32, G, POINTER(c_int32)]),
         "ecl_heuristic_threshold": (c_int, [G, POINTER(c_int32), POINTER(c_int32)]),
         "ecl_default_opts": (None, [POINTER(MstOpts)]),
         "ecl_mst_run": (c_int, [G, c_void_p, POINTER(MstOpts), POINTER(MstStats)]),
@@ -223,6 +224,23 @@ def gen_rgg2d(nodes, avg_degree, seed, wmax, threads=0):
     gc = EclGraphC()
     _check(load().ecl_gen_rgg2d(nodes, avg_degree, seed, wmax, threads, ctypes.byref(gc)), "gen_rgg2d")
     return Graph._from_c(gc)
+
+
+def gen_batch_graph(index, seed0=1000, nmin=1000, nmax=2_000_000, wmax=1 << 20):
+    """Graph `index` of the mixed-family batch; returns (Graph, family 0..3)."""
+    gc = EclGraphC()
+    fam = c_int32()
+    _check(load().ecl_gen_batch_graph(index, seed0, nmin, nmax, wmax, ctypes.byref(gc), ctypes.byref(fam)),
+           "gen_batch_graph")
+    return Graph._from_c(gc), fam.value
+
+
+def gen_batch(count, seed0=1000, nmin=1000, nmax=2_000_000, wmax=1 << 20, threads=0):
+    """The first `count` graphs of the mixed batch, generated in parallel."""
+    from concurrent.futures import ThreadPoolExecutor
+    workers = threads or os.cpu_count() or 1
+    with ThreadPoolExecutor(workers) as ex:
+        return list(ex.map(lambda i: gen_batch_graph(i, seed0, nmin, nmax, wmax)[0], range(count)))
 
 
 def heuristic_threshold(g):
