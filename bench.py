@@ -75,7 +75,7 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 20 ms during the timed region."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -92,7 +92,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "20"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
         return self
@@ -181,7 +181,7 @@ def batch_leg(args, E, torch, dev):
     ew = torch.from_numpy(b.eweight).to(dev)
     out = torch.zeros(b.total_edges, dtype=torch.uint8, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    bc = E.BatchContext(len(graphs), int(b.nodes.max()), int(b.edges.max()), 1 << 19)
+    bc = E.BatchContext(len(graphs), int(b.nodes.max()), int(b.edges.max()), 1 << 21)
     stream = torch.cuda.current_stream(dev).cuda_stream
     best, tune_ms = bc.autotune(b, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr())
     for _ in range(2):
@@ -197,6 +197,7 @@ def batch_leg(args, E, torch, dev):
     res = {"graphs": len(graphs), "edges": total_m, "ms": t, "graphs_per_s": len(graphs) / (t * 1e-3),
            "gedges_per_s": total_m / (t * 1e-3) / 1e9, "graphs_small": last["graphs_small"],
            "graphs_large": last["graphs_large"], "cuda_graph_replay": last["graph_replay"],
+           "ms_small": last["ms_small"], "ms_large": last["ms_large"],
            "autotuned": {"batch_small_edges": best.batch_small_edges, "degree_split": best.degree_split,
                          "small_tail": best.small_tail},
            "gen_s": round(gen_s, 1),

@@ -285,6 +285,40 @@ int ecl_mst_run_batch_device(ecl_batch_ctx* ctx, const ecl_batch* batch,
 int ecl_batch_autotune(ecl_batch_ctx* ctx, const ecl_batch* batch, uint8_t* d_inMST,
                        const mst_opts* base, mst_opts* best, float* best_ms);
 
+/* ---------------------------------------------------- learned schedule */
+/* A 16 -> 64 -> 64 -> 2 ReLU MLP (fp32) maps 16 graph features to the light-
+ * phase filter quantile (output 0, log2 q; >= 0 means no filter) and the
+ * scans' degree split (output 1, log2 split). It changes the schedule only.
+ * Parameter blob (ECL_MLP_PARAMS floats): W1[16][64], b1[64], W2[64][64],
+ * b2[64], W3[64][2], b3[2], feature mean[16], feature std[16]. */
+#define ECL_MLP_INPUTS 16
+#define ECL_MLP_HIDDEN 64
+#define ECL_MLP_OUTPUTS 2
+#define ECL_MLP_PARAMS 5410
+
+/* Load the weights used by ECL_THRESH_LEARNED (process-wide). Without
+ * weights, ECL_THRESH_LEARNED falls back to the reference heuristic. */
+int ecl_learned_set_weights(const float* params, int count);
+int ecl_learned_has_weights(void);
+
+/* The 16 features of a device-resident graph (computed on the device):
+ * log2 n, log2 m, log2(avg degree + 1), log2(max degree + 1), degree CV,
+ * fractions of vertices with degree 0, < 4, >= 32, 3n/m, and the 1, 2, 5,
+ * 10, 20, 30, 50 % quantiles of a 4096-entry weight sample over its max. */
+int ecl_graph_features(const ecl_graph* d_graph, float* out16);
+
+/* MLP kernels on the current device, host buffers in and out:
+ * forward (B samples of raw features -> B x 2 outputs), full-batch
+ * mean-squared-error gradient of W1..b3 (5378 floats; inputs already
+ * standardised), and a whole Adam training run in one launch (minibatches of
+ * 64 standardised samples, in the given order; params updated in place;
+ * loss_hist gets one mean loss per epoch). */
+int ecl_mlp_forward(const float* params, const float* x, int B, float* y);
+int ecl_mlp_grad(const float* params, const float* x, const float* t, int B,
+                 float* grad, float* loss);
+int ecl_mlp_train(float* params, const float* x, const float* t, int B,
+                  int epochs, float lr, float* loss_hist);
+
 /* Wait for the context's stream and report a device-side error if any. */
 int ecl_mst_ctx_sync(ecl_mst_ctx* ctx);
 

@@ -47,6 +47,10 @@ struct ecl_mst_ctx {
   int* d_eweight = nullptr;
   unsigned char* d_inMST = nullptr;
   cudaEvent_t ev[5] = {};
+  // learned schedule: MLP parameters, the 16 features, degree accumulators
+  float* ml_params = nullptr;
+  float* ml_feat = nullptr;
+  void* ml_acc = nullptr;
 };
 
 namespace {
@@ -126,6 +130,9 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   c->first_v_cap = (int)(max_edges / kGran + 2);
   if ((st = cuda_status(cudaMalloc(&c->first_v, (size_t)c->first_v_cap * sizeof(int))))) return fail(st);
   if ((st = cuda_status(cudaMalloc(&c->st, sizeof(DevState))))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->ml_params, ECL_MLP_PARAMS * sizeof(float))))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->ml_feat, ECL_MLP_INPUTS * sizeof(float))))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->ml_acc, 64)))) return fail(st);
   if ((st = cuda_status(cudaHostAlloc(&c->st_host, sizeof(DevState), cudaHostAllocDefault))))
     return fail(st);
   for (auto& e : c->ev)
@@ -144,6 +151,9 @@ extern "C" void ecl_mst_ctx_destroy(ecl_mst_ctx* c) {
   cudaFree(c->wl[0]);
   cudaFree(c->wl[1]);
   cudaFree(c->first_v);
+  cudaFree(c->ml_params);
+  cudaFree(c->ml_feat);
+  cudaFree(c->ml_acc);
   cudaFree(c->st);
   cudaFreeHost(c->st_host);
   cudaFree(c->d_nindex);
@@ -333,6 +343,14 @@ int check_opts(const mst_opts* o) {
 // trained MLP, writing DevState::quantile and DevState::learned_split.
 int ecl_learned_prepare(ecl_mst_ctx* c, const ecl_graph* d_graph, cudaStream_t s, void* st);
 
+int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, float** feat, void** acc, int* sm_count) {
+  *params = c->ml_params;
+  *feat = c->ml_feat;
+  *acc = c->ml_acc;
+  *sm_count = c->sm_count;
+  return ECL_OK;
+}
+
 extern "C" int ecl_mst_run_device(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d_inMST,
                                   const mst_opts* opts, void* stream, ecl_mst_stats* stats) {
   int st = check_graph_args(c, g, d_inMST);
@@ -352,7 +370,9 @@ extern "C" int ecl_mst_run_device(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d
   }
   ECL_CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevState), s));
   if (o.threshold_mode == ECL_THRESH_LEARNED) {
-    if ((st = ecl_learned_prepare(c, g, s, c->st))) return st;
+    st = ecl_learned_prepare(c, g, s, c->st);
+    if (st == ECL_ERR_UNSUPPORTED) o.threshold_mode = ECL_THRESH_HEURISTIC;  // no weights loaded
+    else if (st) return st;
   }
   if ((st = enqueue_solve(c, g, d_inMST, &o, s, stats != nullptr))) return st;
   if (stats) {
@@ -879,7 +899,7 @@ extern "C" int ecl_batch_autotune(ecl_batch_ctx* c, const ecl_batch* b, uint8_t*
   else ecl_default_opts(&o0);
   float best_t = 1e30f;
   mst_opts best_o = o0;
-  const int cutoffs[] = {c->cap / 8, c->cap / 2, c->cap};
+  const int cutoffs[] = {c->cap / 8, c->cap / 4, c->cap / 2, c->cap};
   const int splits[] = {8, 16};
   const int tails[] = {4096, 16384};
   for (int cut : cutoffs) {

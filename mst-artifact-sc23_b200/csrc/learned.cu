@@ -1,9 +1,415 @@
-// Learned filter threshold and degree split (placeholder until the MLP lands).
+// Learned schedule for the MST solve: graph features computed on the device,
+// and a small MLP (16 -> 64 -> 64 -> 2, ReLU, fp32) with hand-written CUDA
+// inference, gradient and training (Adam) kernels. The network maps the
+// features to the light-phase filter quantile (output 0, as log2 q) and the
+// scan's degree split (output 1, as log2 split). Only the schedule changes;
+// the forest is unique under the (weight, index) order, so the answer does
+// not (for non-negative weights). The reference heuristic (ECL_MST.cu:432-440)
+// remains the fallback when no weights are loaded.
+//
+// Parameter blob layout (kMlpParams floats):
+//   W1[16][64], b1[64], W2[64][64], b2[64], W3[64][2], b3[2], mean[16], std[16]
+// Features are standardised with mean/std before the first layer.
 #include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "ecl_mst.h"
+#include "internal.h"
+#include "mst_kernels.cuh"
+
+namespace {
+
+constexpr int kIn = ECL_MLP_INPUTS, kH = ECL_MLP_HIDDEN, kOut = ECL_MLP_OUTPUTS;
+constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kIn * kH, kOffW2 = kOffB1 + kH, kOffB2 = kOffW2 + kH * kH;
+constexpr int kOffW3 = kOffB2 + kH, kOffB3 = kOffW3 + kH * kOut, kOffMean = kOffB3 + kOut;
+constexpr int kOffStd = kOffMean + kIn, kParams = kOffStd + kIn;
+static_assert(kParams == ECL_MLP_PARAMS, "parameter blob size");
+constexpr int kTrainable = kOffMean;  // W1..b3
+constexpr int kMB = 64;               // training minibatch
+constexpr int kSample = 4096;         // weight sample for the quantile features
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return ECL_OK;
+  if (e == cudaErrorMemoryAllocation) return ECL_ERR_ALLOC;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return ECL_ERR_NO_DEVICE;
+  return ECL_ERR_CUDA;
+}
+#define ML_TRY(call)                               \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) return cuda_status(e_); \
+  } while (0)
+
+// ------------------------------------------------------------- features
+struct FeatAcc {
+  unsigned long long deg_sum, deg_sq, zero, low, high;
+  unsigned max_deg;
+};
+
+// Degree statistics over all vertices (grid-stride, block reduction, one
+// atomic per block per counter).
+__global__ void k_feat_degrees(const int* nindex, int n, FeatAcc* acc) {
+  __shared__ unsigned long long s[5][32];
+  __shared__ unsigned smax[32];
+  unsigned long long d1 = 0, d2 = 0, z = 0, lo = 0, hi = 0;
+  unsigned mx = 0;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const int d = __ldg(nindex + v + 1) - __ldg(nindex + v);
+    const unsigned ud = d > 0 ? (unsigned)d : 0u;
+    d1 += ud;
+    d2 += (unsigned long long)ud * ud;
+    z += ud == 0;
+    lo += ud < 4;
+    hi += ud >= 32;
+    mx = max(mx, ud);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    d1 += __shfl_down_sync(0xffffffffu, d1, o);
+    d2 += __shfl_down_sync(0xffffffffu, d2, o);
+    z += __shfl_down_sync(0xffffffffu, z, o);
+    lo += __shfl_down_sync(0xffffffffu, lo, o);
+    hi += __shfl_down_sync(0xffffffffu, hi, o);
+    mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  }
+  if (lane == 0) {
+    s[0][w] = d1;
+    s[1][w] = d2;
+    s[2][w] = z;
+    s[3][w] = lo;
+    s[4][w] = hi;
+    smax[w] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < (int)(blockDim.x >> 5); i++) {
+      for (int k = 0; k < 5; k++) s[k][0] += s[k][i];
+      smax[0] = max(smax[0], smax[i]);
+    }
+    atomicAdd(&acc->deg_sum, s[0][0]);
+    atomicAdd(&acc->deg_sq, s[1][0]);
+    atomicAdd(&acc->zero, s[2][0]);
+    atomicAdd(&acc->low, s[3][0]);
+    atomicAdd(&acc->high, s[4][0]);
+    atomicMax(&acc->max_deg, smax[0]);
+  }
+}
+
+// The 16 features, from the degree statistics and a sorted 4096-entry weight
+// sample (one CTA of 1024 threads).
+__global__ void k_feat_finish(const int* eweight, int n, int m, const FeatAcc* acc, float* out) {
+  __shared__ int samp[kSample];
+  for (int i = threadIdx.x; i < kSample; i += blockDim.x) {
+    const uint64_t r = ecl_mix64(0xFEA70000ull + (uint64_t)i);
+    samp[i] = m > 0 ? eweight[(unsigned)(r % (uint64_t)(unsigned)m)] : 0;
+  }
+  __syncthreads();
+  for (int k = 2; k <= kSample; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < kSample; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const int x = samp[i], y = samp[ixj];
+          if ((x > y) == ((i & k) == 0)) {
+            samp[i] = y;
+            samp[ixj] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  if (threadIdx.x != 0) return;
+  const double dn = (double)n, dm = (double)m;
+  const double mean = dm / dn;
+  const double var = fmax(0.0, (double)acc->deg_sq / dn - mean * mean);
+  const double wmax = fmax(1.0, (double)samp[kSample - 1]);
+  const float qs[7] = {0.01f, 0.02f, 0.05f, 0.1f, 0.2f, 0.3f, 0.5f};
+  out[0] = (float)log2(dn);
+  out[1] = (float)log2(fmax(dm, 1.0));
+  out[2] = (float)log2(mean + 1.0);
+  out[3] = (float)log2((double)acc->max_deg + 1.0);
+  out[4] = (float)(sqrt(var) / fmax(mean, 1e-9));
+  out[5] = (float)((double)acc->zero / dn);
+  out[6] = (float)((double)acc->low / dn);
+  out[7] = (float)((double)acc->high / dn);
+  out[8] = (float)(3.0 * dn / fmax(dm, 1.0));  // the reference heuristic's "300% of nodes" quantile
+  for (int i = 0; i < 7; i++) out[9 + i] = (float)((double)samp[(int)(qs[i] * (kSample - 1))] / wmax);
+}
+
+// ------------------------------------------------------------------- MLP
+__device__ __forceinline__ float relu(float x) { return x > 0.f ? x : 0.f; }
+
+// Forward pass of one sample held in x[kIn] (already standardised); h1, h2
+// and y are written. Serial per thread (the network is tiny).
+__device__ void mlp_forward1(const float* p, const float* x, float* h1, float* h2, float* y) {
+  for (int j = 0; j < kH; j++) {
+    float a = p[kOffB1 + j];
+    for (int i = 0; i < kIn; i++) a += x[i] * p[kOffW1 + i * kH + j];
+    h1[j] = relu(a);
+  }
+  for (int k = 0; k < kH; k++) {
+    float a = p[kOffB2 + k];
+    for (int j = 0; j < kH; j++) a += h1[j] * p[kOffW2 + j * kH + k];
+    h2[k] = relu(a);
+  }
+  for (int o = 0; o < kOut; o++) {
+    float a = p[kOffB3 + o];
+    for (int k = 0; k < kH; k++) a += h2[k] * p[kOffW3 + k * kOut + o];
+    y[o] = a;
+  }
+}
+
+// Inference for B samples (raw features; standardised here).
+__global__ void k_mlp_infer(const float* p, const float* x, int B, float* y) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  float xs[kIn], h1[kH], h2[kH];
+  for (int i = 0; i < kIn; i++) xs[i] = (x[b * kIn + i] - p[kOffMean + i]) / p[kOffStd + i];
+  mlp_forward1(p, xs, h1, h2, y + b * kOut);
+}
+
+// Decode the network output into the solve's control block.
+__global__ void k_mlp_apply(const float* p, const float* feat, ecl::DevState* st) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  float xs[kIn], h1[kH], h2[kH], y[kOut];
+  for (int i = 0; i < kIn; i++) xs[i] = (feat[i] - p[kOffMean + i]) / p[kOffStd + i];
+  mlp_forward1(p, xs, h1, h2, y);
+  // output 0: log2 of the filter quantile; >= -0.02 means "no filter"
+  const float lq = fminf(fmaxf(y[0], -10.f), 0.f);
+  st->quantile = lq >= -0.02f ? 1.0f : exp2f(lq);
+  // output 1: log2 of the degree split, in [1, 6]
+  const int ls = (int)lrintf(fminf(fmaxf(y[1], 1.f), 6.f));
+  st->learned_split = 1 << ls;
+}
+
+// Full-batch mean-squared-error loss and gradient of the trainable
+// parameters (W1..b3). One CTA; every thread accumulates the gradient of a
+// strided subset of samples into shared memory with atomics, in a fixed
+// order per thread. grad must hold kTrainable floats.
+__device__ void mlp_grad_block(const float* p, const float* x, const float* t, int B, float* g_sm,
+                               float* loss_sm) {
+  for (int i = threadIdx.x; i < kTrainable; i += blockDim.x) g_sm[i] = 0.f;
+  if (threadIdx.x == 0) *loss_sm = 0.f;
+  __syncthreads();
+  const float inv = 1.f / (float)(B > 0 ? B : 1);
+  for (int b = threadIdx.x; b < B; b += blockDim.x) {
+    float xs[kIn], h1[kH], h2[kH], y[kOut], dy[kOut], d2[kH];
+    for (int i = 0; i < kIn; i++) xs[i] = x[b * kIn + i];
+    mlp_forward1(p, xs, h1, h2, y);
+    float l = 0.f;
+    for (int o = 0; o < kOut; o++) {
+      const float e = y[o] - t[b * kOut + o];
+      l += e * e;
+      dy[o] = 2.f * e * inv;
+    }
+    atomicAdd(loss_sm, l * inv);
+    for (int o = 0; o < kOut; o++) atomicAdd(&g_sm[kOffB3 + o], dy[o]);
+    for (int k = 0; k < kH; k++) {
+      float a = 0.f;
+      for (int o = 0; o < kOut; o++) {
+        atomicAdd(&g_sm[kOffW3 + k * kOut + o], h2[k] * dy[o]);
+        a += dy[o] * p[kOffW3 + k * kOut + o];
+      }
+      d2[k] = h2[k] > 0.f ? a : 0.f;
+      atomicAdd(&g_sm[kOffB2 + k], d2[k]);
+    }
+    for (int j = 0; j < kH; j++) {
+      float a = 0.f;
+      for (int k = 0; k < kH; k++) {
+        if (d2[k] != 0.f) atomicAdd(&g_sm[kOffW2 + j * kH + k], h1[j] * d2[k]);
+        a += d2[k] * p[kOffW2 + j * kH + k];
+      }
+      const float d1 = h1[j] > 0.f ? a : 0.f;
+      if (d1 != 0.f) {
+        atomicAdd(&g_sm[kOffB1 + j], d1);
+        for (int i = 0; i < kIn; i++) atomicAdd(&g_sm[kOffW1 + i * kH + j], xs[i] * d1);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+__global__ void k_mlp_grad(const float* p, const float* x, const float* t, int B, float* grad,
+                           float* loss) {
+  extern __shared__ float smem[];
+  float* g_sm = smem;
+  float* l_sm = smem + kTrainable;
+  mlp_grad_block(p, x, t, B, g_sm, l_sm);
+  for (int i = threadIdx.x; i < kTrainable; i += blockDim.x) grad[i] = g_sm[i];
+  if (threadIdx.x == 0) *loss = *l_sm;
+}
+
+// The whole training run in one launch (one CTA): epochs over minibatches
+// of kMB standardised samples, Adam (beta1 0.9, beta2 0.999, eps 1e-8).
+// Parameters and the two moment vectors live in global memory; gradients in
+// shared memory. loss_hist[e] = mean minibatch loss of epoch e.
+__global__ void k_mlp_train(float* p, float* m1, float* m2, const float* x, const float* t, int B,
+                            int epochs, float lr, float* loss_hist) {
+  extern __shared__ float smem[];
+  float* g_sm = smem;
+  float* l_sm = smem + kTrainable;
+  int step = 0;
+  for (int e = 0; e < epochs; e++) {
+    float acc = 0.f;
+    int nb = 0;
+    for (int b0 = 0; b0 < B; b0 += kMB) {
+      const int bs = min(kMB, B - b0);
+      mlp_grad_block(p, x + (size_t)b0 * kIn, t + (size_t)b0 * kOut, bs, g_sm, l_sm);
+      step++;
+      const float c1 = 1.f - powf(0.9f, (float)step), c2 = 1.f - powf(0.999f, (float)step);
+      for (int i = threadIdx.x; i < kTrainable; i += blockDim.x) {
+        const float g = g_sm[i];
+        const float a = 0.9f * m1[i] + 0.1f * g;
+        const float v = 0.999f * m2[i] + 0.001f * g * g;
+        m1[i] = a;
+        m2[i] = v;
+        p[i] -= lr * (a / c1) / (sqrtf(v / c2) + 1e-8f);
+      }
+      acc += *l_sm;
+      nb++;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) loss_hist[e] = acc / (float)(nb > 0 ? nb : 1);
+    __syncthreads();
+  }
+}
+
+std::mutex g_w_mu;
+std::vector<float> g_weights;  // host copy of the loaded parameter blob
+
+}  // namespace
 
 struct ecl_mst_ctx;
-int ecl_learned_prepare(ecl_mst_ctx*, const ecl_graph*, cudaStream_t, void*) {
-  return ECL_ERR_UNSUPPORTED;
+int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, float** feat, void** acc, int* sm_count);
+
+extern "C" int ecl_learned_set_weights(const float* params, int count) {
+  if (count != kParams || !params) return ECL_ERR_INVALID_ARG;
+  for (int i = 0; i < kIn; i++)
+    if (!(params[kOffStd + i] > 0.f)) return ECL_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(g_w_mu);
+  g_weights.assign(params, params + count);
+  return ECL_OK;
+}
+
+extern "C" int ecl_learned_has_weights(void) {
+  std::lock_guard<std::mutex> lock(g_w_mu);
+  return g_weights.empty() ? 0 : 1;
+}
+
+// Features + MLP on the device for the learned schedule; writes the decoded
+// quantile and split into the solve's control block. Returns
+// ECL_ERR_UNSUPPORTED when no weights are loaded (the caller then falls back
+// to the reference heuristic).
+int ecl_learned_prepare(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s, void* st) {
+  std::vector<float> w;
+  {
+    std::lock_guard<std::mutex> lock(g_w_mu);
+    w = g_weights;
+  }
+  if (w.empty()) return ECL_ERR_UNSUPPORTED;
+  float *d_params, *d_feat;
+  void* d_acc;
+  int sms = 0;
+  int r = ecl_ctx_learned_buffers(c, &d_params, &d_feat, &d_acc, &sms);
+  if (r) return r;
+  ML_TRY(cudaMemcpyAsync(d_params, w.data(), kParams * sizeof(float), cudaMemcpyHostToDevice, s));
+  ML_TRY(cudaMemsetAsync(d_acc, 0, sizeof(FeatAcc), s));
+  const int grid = std::max(1, std::min(sms * 4, (g->nodes + 511) / 512));
+  k_feat_degrees<<<grid, 512, 0, s>>>(g->nindex, g->nodes, (FeatAcc*)d_acc);
+  k_feat_finish<<<1, 1024, 0, s>>>(g->eweight, g->nodes, g->edges, (const FeatAcc*)d_acc, d_feat);
+  k_mlp_apply<<<1, 32, 0, s>>>(d_params, d_feat, (ecl::DevState*)st);
+  ML_TRY(cudaGetLastError());
+  return ECL_OK;
+}
+
+// Features of a device-resident graph, copied to host out[16].
+extern "C" int ecl_graph_features(const ecl_graph* g, float* out) {
+  if (!g || !out || g->nodes < 1 || g->edges < 0 || !g->nindex || (g->edges > 0 && !g->eweight))
+    return ECL_ERR_INVALID_ARG;
+  int dev = 0, sms = 0;
+  ML_TRY(cudaGetDevice(&dev));
+  ML_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  FeatAcc* acc = nullptr;
+  float* f = nullptr;
+  ML_TRY(cudaMalloc(&acc, sizeof(FeatAcc)));
+  if (cudaMalloc(&f, kIn * sizeof(float)) != cudaSuccess) {
+    cudaFree(acc);
+    return ECL_ERR_ALLOC;
+  }
+  cudaMemset(acc, 0, sizeof(FeatAcc));
+  const int grid = std::max(1, std::min(sms * 4, (g->nodes + 511) / 512));
+  k_feat_degrees<<<grid, 512>>>(g->nindex, g->nodes, acc);
+  k_feat_finish<<<1, 1024>>>(g->eweight, g->nodes, g->edges, acc, f);
+  cudaError_t e = cudaMemcpy(out, f, kIn * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(acc);
+  cudaFree(f);
+  return cuda_status(e);
+}
+
+namespace {
+struct DevBuf {
+  float* p = nullptr;
+  ~DevBuf() { cudaFree(p); }
+  int alloc(size_t n) { return cuda_status(cudaMalloc(&p, n * sizeof(float))); }
+};
+}  // namespace
+
+extern "C" int ecl_mlp_forward(const float* params, const float* x, int B, float* y) {
+  if (!params || !x || !y || B < 0) return ECL_ERR_INVALID_ARG;
+  if (B == 0) return ECL_OK;
+  DevBuf dp, dx, dy;
+  int r;
+  if ((r = dp.alloc(kParams)) || (r = dx.alloc((size_t)B * kIn)) || (r = dy.alloc((size_t)B * kOut))) return r;
+  ML_TRY(cudaMemcpy(dp.p, params, kParams * sizeof(float), cudaMemcpyHostToDevice));
+  ML_TRY(cudaMemcpy(dx.p, x, (size_t)B * kIn * sizeof(float), cudaMemcpyHostToDevice));
+  k_mlp_infer<<<(B + 127) / 128, 128>>>(dp.p, dx.p, B, dy.p);
+  ML_TRY(cudaGetLastError());
+  ML_TRY(cudaMemcpy(y, dy.p, (size_t)B * kOut * sizeof(float), cudaMemcpyDeviceToHost));
+  return ECL_OK;
+}
+
+extern "C" int ecl_mlp_grad(const float* params, const float* x, const float* t, int B, float* grad,
+                            float* loss) {
+  if (!params || !x || !t || !grad || !loss || B < 1) return ECL_ERR_INVALID_ARG;
+  DevBuf dp, dx, dt, dg, dl;
+  int r;
+  if ((r = dp.alloc(kParams)) || (r = dx.alloc((size_t)B * kIn)) || (r = dt.alloc((size_t)B * kOut)) ||
+      (r = dg.alloc(kTrainable)) || (r = dl.alloc(1)))
+    return r;
+  ML_TRY(cudaMemcpy(dp.p, params, kParams * sizeof(float), cudaMemcpyHostToDevice));
+  ML_TRY(cudaMemcpy(dx.p, x, (size_t)B * kIn * sizeof(float), cudaMemcpyHostToDevice));
+  ML_TRY(cudaMemcpy(dt.p, t, (size_t)B * kOut * sizeof(float), cudaMemcpyHostToDevice));
+  const size_t smem = (kTrainable + 1) * sizeof(float);
+  ML_TRY(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_mlp_grad<<<1, 256, smem>>>(dp.p, dx.p, dt.p, B, dg.p, dl.p);
+  ML_TRY(cudaGetLastError());
+  ML_TRY(cudaMemcpy(grad, dg.p, kTrainable * sizeof(float), cudaMemcpyDeviceToHost));
+  ML_TRY(cudaMemcpy(loss, dl.p, sizeof(float), cudaMemcpyDeviceToHost));
+  return ECL_OK;
+}
+
+extern "C" int ecl_mlp_train(float* params, const float* x, const float* t, int B, int epochs, float lr,
+                             float* loss_hist) {
+  if (!params || !x || !t || B < 1 || epochs < 1 || !(lr > 0.f)) return ECL_ERR_INVALID_ARG;
+  DevBuf dp, dm1, dm2, dx, dt, dl;
+  int r;
+  if ((r = dp.alloc(kParams)) || (r = dm1.alloc(kTrainable)) || (r = dm2.alloc(kTrainable)) ||
+      (r = dx.alloc((size_t)B * kIn)) || (r = dt.alloc((size_t)B * kOut)) || (r = dl.alloc(epochs)))
+    return r;
+  ML_TRY(cudaMemcpy(dp.p, params, kParams * sizeof(float), cudaMemcpyHostToDevice));
+  ML_TRY(cudaMemset(dm1.p, 0, kTrainable * sizeof(float)));
+  ML_TRY(cudaMemset(dm2.p, 0, kTrainable * sizeof(float)));
+  ML_TRY(cudaMemcpy(dx.p, x, (size_t)B * kIn * sizeof(float), cudaMemcpyHostToDevice));
+  ML_TRY(cudaMemcpy(dt.p, t, (size_t)B * kOut * sizeof(float), cudaMemcpyHostToDevice));
+  const size_t smem = (kTrainable + 1) * sizeof(float);
+  ML_TRY(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_mlp_train<<<1, 256, smem>>>(dp.p, dm1.p, dm2.p, dx.p, dt.p, B, epochs, lr, dl.p);
+  ML_TRY(cudaGetLastError());
+  ML_TRY(cudaMemcpy(params, dp.p, kParams * sizeof(float), cudaMemcpyDeviceToHost));
+  if (loss_hist) ML_TRY(cudaMemcpy(loss_hist, dl.p, (size_t)epochs * sizeof(float), cudaMemcpyDeviceToHost));
+  return ECL_OK;
 }

@@ -129,6 +129,12 @@ def load():
                                              POINTER(BatchStats)]),
         "ecl_batch_autotune": (c_int, [c_void_p, POINTER(EclBatchC), c_void_p, POINTER(MstOpts), POINTER(MstOpts),
                                        POINTER(c_float)]),
+        "ecl_learned_set_weights": (c_int, [c_void_p, c_int]),
+        "ecl_learned_has_weights": (c_int, []),
+        "ecl_graph_features": (c_int, [G, c_void_p]),
+        "ecl_mlp_forward": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+        "ecl_mlp_grad": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, POINTER(c_float)]),
+        "ecl_mlp_train": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_float, c_void_p]),
         "ecl_verify": (c_int, [G, c_void_p, c_void_p, POINTER(c_int64), POINTER(c_uint64), POINTER(c_uint64)]),
         "ecl_forest_weight": (c_uint64, [G, c_void_p]),
     }
@@ -424,3 +430,73 @@ class BatchContext:
                                             None if base is None else ctypes.byref(base), ctypes.byref(best),
                                             ctypes.byref(ms)), "batch_autotune")
         return best, ms.value
+
+
+# ----------------------------------------------------------- learned schedule
+MLP_IN, MLP_H, MLP_OUT = 16, 64, 2
+MLP_PARAMS = MLP_IN * MLP_H + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H * MLP_OUT + MLP_OUT + 2 * MLP_IN
+MLP_TRAINABLE = MLP_PARAMS - 2 * MLP_IN
+WEIGHTS_PATH = os.path.join(_HERE, "filter_weights.bin")
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def mlp_init(seed=0, mean=None, std=None):
+    """He-initialised parameter blob (W1, b1, W2, b2, W3, b3, mean, std)."""
+    rng = np.random.default_rng(seed)
+    parts = [rng.normal(0, np.sqrt(2 / MLP_IN), MLP_IN * MLP_H), np.zeros(MLP_H),
+             rng.normal(0, np.sqrt(2 / MLP_H), MLP_H * MLP_H), np.zeros(MLP_H),
+             rng.normal(0, np.sqrt(1 / MLP_H), MLP_H * MLP_OUT), np.zeros(MLP_OUT),
+             np.zeros(MLP_IN) if mean is None else mean, np.ones(MLP_IN) if std is None else std]
+    return _f32(np.concatenate(parts))
+
+
+def mlp_forward(params, x):
+    """CUDA inference: raw features (B x 16) -> outputs (B x 2)."""
+    params, x = _f32(params), _f32(x)
+    y = np.zeros((x.shape[0], MLP_OUT), np.float32)
+    _check(load().ecl_mlp_forward(_ptr(params), _ptr(x), x.shape[0], _ptr(y)), "mlp_forward")
+    return y
+
+
+def mlp_grad(params, x, t):
+    """CUDA full-batch MSE gradient of W1..b3 (standardised inputs)."""
+    params, x, t = _f32(params), _f32(x), _f32(t)
+    g = np.zeros(MLP_TRAINABLE, np.float32)
+    loss = c_float()
+    _check(load().ecl_mlp_grad(_ptr(params), _ptr(x), _ptr(t), x.shape[0], _ptr(g), ctypes.byref(loss)),
+           "mlp_grad")
+    return g, loss.value
+
+
+def mlp_train(params, x, t, epochs, lr):
+    """CUDA Adam training run (standardised inputs); returns (params, loss per epoch)."""
+    params = _f32(params).copy()
+    x, t = _f32(x), _f32(t)
+    hist = np.zeros(epochs, np.float32)
+    _check(load().ecl_mlp_train(_ptr(params), _ptr(x), _ptr(t), x.shape[0], epochs, lr, _ptr(hist)),
+           "mlp_train")
+    return params, hist
+
+
+def graph_features(nodes, edges, d_nindex, d_nlist, d_eweight):
+    """The 16 schedule features of a device-resident graph (computed on the GPU)."""
+    out = np.zeros(MLP_IN, np.float32)
+    gs = EclGraphC(nodes, edges, d_nindex, d_nlist, d_eweight)
+    _check(load().ecl_graph_features(ctypes.byref(gs), _ptr(out)), "graph_features")
+    return out
+
+
+def learned_set_weights(params):
+    params = _f32(params)
+    _check(load().ecl_learned_set_weights(_ptr(params), params.size), "learned_set_weights")
+
+
+def learned_load_default():
+    """Load the trained weights shipped next to this module; False if absent."""
+    if not os.path.exists(WEIGHTS_PATH):
+        return False
+    learned_set_weights(np.fromfile(WEIGHTS_PATH, np.float32))
+    return True

@@ -1,0 +1,151 @@
+"""Training pipeline of the learned schedule (runs on a GPU).
+
+1. Generate seeded training and held-out graphs from the four families
+   (2D grid, Erdos-Renyi avg degree 8-32, RMAT (.57,.19,.19) edge factor 8-32,
+   random geometric 2D avg degree 3), vertex counts log-uniform in
+   [--nmin, --nmax].
+2. Label sweep: solve every graph with each of 16 filter quantiles x 6 degree
+   splits (device time, best of --reps runs) and take the fastest setting
+   as the label (log2 quantile, log2 split). The sweep uses the engine's own
+   schedules; every setting gives the same forest.
+3. Train the 16 -> 64 -> 64 -> 2 MLP with the library's CUDA training kernel
+   (Adam, one launch) on standardised features.
+4. Evaluate on the held-out graphs: device time of the learned schedule vs
+   the reference heuristic (its fallback and judge) vs the best of the sweep.
+5. Write the parameter blob (filter_weights.bin, next to this file unless
+   --out says otherwise) and a JSON summary.
+
+    python train_filter.py --train 600 --heldout 100 --out-dir <dir>
+"""
+import argparse
+import json
+import os
+import sys
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import ecl_mst as E  # noqa: E402
+
+QUANTILES = [0.005, 0.01, 0.02, 0.03, 0.05, 0.07, 0.1, 0.15, 0.2, 0.3, 0.4, 0.5, 0.65, 0.8, 0.9, 1.0]
+SPLITS = [2, 4, 8, 16, 32, 64]
+
+
+def make_graph(seed, nmin, nmax):
+    rng = np.random.default_rng(seed)
+    fam = int(rng.integers(4))
+    n = int(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
+    if fam == 0:
+        r = max(2, int(np.sqrt(n)))
+        return E.gen_grid(r, max(2, n // r), seed, 1 << 24, threads=2), "grid"
+    if fam == 1:
+        return E.gen_er(n, float(rng.choice([8, 16, 32])), seed, 1 << 24, threads=2), "er"
+    if fam == 2:
+        return E.gen_rmat(max(10, int(round(np.log2(n)))), int(rng.choice([8, 16, 32])), 0.57, 0.19, 0.19, seed,
+                          1 << 24, threads=2), "rmat"
+    return E.gen_rgg2d(n, 3.0, seed, 1 << 24, threads=2), "rgg"
+
+
+def sweep(ctx, g, torch, dev, reps):
+    ni, nl, ew = (torch.from_numpy(a).to(dev) for a in (g.nindex, g.nlist, g.eweight))
+    out = torch.empty(max(g.edges, 1), dtype=torch.uint8, device=dev)
+    feat = E.graph_features(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), ew.data_ptr())
+
+    def timed(opts):
+        best = 1e30
+        for r in range(reps + 1):
+            st = ctx.run_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(),
+                                opts=opts, stats=True)
+            if r > 0:
+                best = min(best, st["ms_total"])
+        return best
+
+    times = np.zeros((len(QUANTILES), len(SPLITS)), np.float32)
+    for qi, q in enumerate(QUANTILES):
+        for si, sp in enumerate(SPLITS):
+            times[qi, si] = timed(E.make_opts(mode=E.THRESH_QUANTILE, quantile=q, degree_split=sp))
+    heur = timed(E.make_opts())
+    learned = timed(E.make_opts(mode=E.THRESH_LEARNED)) if E.learned_load_default() else None
+    return feat, times, heur, learned
+
+
+def label(times):
+    qi, si = np.unravel_index(int(np.argmin(times)), times.shape)
+    return np.array([np.log2(QUANTILES[qi]), np.log2(SPLITS[si])], np.float32)
+
+
+def run(args):
+    import torch
+    dev = torch.device("cuda:0")
+    ctx = E.Context(args.nmax * 2, args.nmax * 130)
+    data = {}
+    for split_name, count, base in (("train", args.train, 200000), ("heldout", args.heldout, 900000)):
+        feats, times, heurs, fams = [], [], [], []
+        t0 = time.time()
+        with ThreadPoolExecutor(max(1, (os.cpu_count() or 2) // 2)) as ex:
+            futs = [ex.submit(make_graph, base + i, args.nmin, args.nmax) for i in range(count)]
+            for i, fu in enumerate(futs):
+                g, fam = fu.result()
+                futs[i] = None
+                f, tm, h, _ = sweep(ctx, g, torch, dev, args.reps)
+                feats.append(f)
+                times.append(tm)
+                heurs.append(h)
+                fams.append(fam)
+        print(f"{split_name}: {count} graphs swept in {time.time() - t0:.0f} s", flush=True)
+        data[split_name] = dict(x=np.array(feats), times=np.array(times), heur=np.array(heurs), fam=fams)
+    ctx.close()
+    tr = data["train"]
+    x = tr["x"]
+    mean, std = x.mean(0), x.std(0) + 1e-6
+    y = np.stack([label(t) for t in tr["times"]])
+    p0 = E.mlp_init(args.seed, mean=mean, std=std)
+    xs = ((x - mean) / std).astype(np.float32)
+    p, hist = E.mlp_train(p0, xs, y, epochs=args.epochs, lr=args.lr)
+    # held-out evaluation from the sweep table: time at the predicted grid point
+    ho = data["heldout"]
+    pred = E.mlp_forward(p, ho["x"])
+    res = []
+    for pr, tm, h in zip(pred, ho["times"], ho["heur"]):
+        lq = min(max(float(pr[0]), -10.0), 0.0)
+        q = 1.0 if lq >= -0.02 else 2.0 ** lq
+        sp = 1 << int(round(min(max(float(pr[1]), 1.0), 6.0)))
+        qi = int(np.argmin([abs(np.log2(a) - np.log2(q)) for a in QUANTILES]))
+        si = SPLITS.index(sp) if sp in SPLITS else 2
+        res.append((float(tm[qi, si]), float(h), float(tm.min())))
+    res = np.array(res)
+    summary = {
+        "train_graphs": args.train, "heldout_graphs": args.heldout, "nmin": args.nmin, "nmax": args.nmax,
+        "quantiles": QUANTILES, "splits": SPLITS, "epochs": args.epochs, "lr": args.lr,
+        "loss_first": float(hist[0]), "loss_last": float(hist[-1]),
+        "heldout_ms_learned": float(res[:, 0].sum()), "heldout_ms_heuristic": float(res[:, 1].sum()),
+        "heldout_ms_best": float(res[:, 2].sum()),
+        "heldout_gain_over_heuristic": float(res[:, 1].sum() / res[:, 0].sum()),
+        "heldout_graphs_not_slower": float((res[:, 0] <= res[:, 1] * 1.02).mean()),
+        "train_label_quantiles": {str(q): int((np.abs(y[:, 0] - np.log2(q)) < 1e-6).sum()) for q in QUANTILES},
+        "train_label_splits": {str(s): int((np.abs(y[:, 1] - np.log2(s)) < 1e-6).sum()) for s in SPLITS},
+    }
+    os.makedirs(args.out_dir, exist_ok=True)
+    np.asarray(p, np.float32).tofile(os.path.join(args.out_dir, "filter_weights.bin"))
+    np.savez_compressed(os.path.join(args.out_dir, "filter_dataset.npz"), train_x=tr["x"], train_times=tr["times"],
+                        train_heur=tr["heur"], heldout_x=ho["x"], heldout_times=ho["times"], heldout_heur=ho["heur"])
+    with open(os.path.join(args.out_dir, "filter_training.json"), "w") as f:
+        json.dump(summary, f, indent=1)
+    print(json.dumps(summary), flush=True)
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", type=int, default=600)
+    ap.add_argument("--heldout", type=int, default=100)
+    ap.add_argument("--nmin", type=int, default=10_000)
+    ap.add_argument("--nmax", type=int, default=1_000_000)
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--epochs", type=int, default=600)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out-dir", default=HERE)
+    run(ap.parse_args())
