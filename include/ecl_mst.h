@@ -287,8 +287,9 @@ int ecl_batch_autotune(ecl_batch_ctx* ctx, const ecl_batch* batch, uint8_t* d_in
 
 /* ---------------------------------------------------- learned schedule */
 /* A 16 -> 64 -> 64 -> 2 ReLU MLP (fp32) maps 16 graph features to the light-
- * phase filter quantile (output 0, log2 q; >= 0 means no filter) and the
- * scans' degree split (output 1, log2 split). It changes the schedule only.
+ * phase filter quantile (output 0: log2 q minus the log2 of the reference
+ * heuristic's quantile, (idx+1)/21 or 1 when it does not filter; a total
+ * >= 0 means no filter) and the scans' degree split (output 1, log2 split). It changes the schedule only.
  * Parameter blob (ECL_MLP_PARAMS floats): W1[16][64], b1[64], W2[64][64],
  * b2[64], W3[64][2], b3[2], feature mean[16], feature std[16]. */
 #define ECL_MLP_INPUTS 16

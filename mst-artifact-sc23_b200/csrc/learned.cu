@@ -1,8 +1,9 @@
 // Learned schedule for the MST solve: graph features computed on the device,
 // and a small MLP (16 -> 64 -> 64 -> 2, ReLU, fp32) with hand-written CUDA
 // inference, gradient and training (Adam) kernels. The network maps the
-// features to the light-phase filter quantile (output 0, as log2 q) and the
-// scan's degree split (output 1, as log2 split). Only the schedule changes;
+// features to the light-phase filter quantile (output 0, as log2 q relative
+// to the reference heuristic's quantile) and the scan's degree split
+// (output 1, as log2 split). Only the schedule changes;
 // the forest is unique under the (weight, index) order, so the answer does
 // not (for non-negative weights). The reference heuristic (ECL_MST.cu:432-440)
 // remains the fallback when no weights are loaded.
@@ -172,14 +173,25 @@ __global__ void k_mlp_infer(const float* p, const float* x, int B, float* y) {
   mlp_forward1(p, xs, h1, h2, y + b * kOut);
 }
 
-// Decode the network output into the solve's control block.
-__global__ void k_mlp_apply(const float* p, const float* feat, ecl::DevState* st) {
+// log2 of the weight quantile the reference heuristic filters at
+// (ECL_MST.cu:408,432-440): the idx-th of 20 samples sits at quantile
+// (idx + 1) / 21 on average; 0 (no filter) when edges/nodes < 4.
+__host__ __device__ __forceinline__ float heuristic_log2_quantile(int n, int m) {
+  if (n < 1 || m / n < 4) return 0.f;
+  const int idx = min(19, (int)(3.0 * n * 20 / m));
+  return log2f((float)(idx + 1) / 21.f);
+}
+
+// Decode the network output into the solve's control block. Output 0 is the
+// log2 quantile relative to the reference heuristic's; output 1 the log2
+// degree split.
+__global__ void k_mlp_apply(const float* p, const float* feat, int n, int m, ecl::DevState* st) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   float xs[kIn], h1[kH], h2[kH], y[kOut];
   for (int i = 0; i < kIn; i++) xs[i] = (feat[i] - p[kOffMean + i]) / p[kOffStd + i];
   mlp_forward1(p, xs, h1, h2, y);
-  // output 0: log2 of the filter quantile; >= -0.02 means "no filter"
-  const float lq = fminf(fmaxf(y[0], -10.f), 0.f);
+  // >= -0.02 means "no filter"
+  const float lq = fminf(fmaxf(heuristic_log2_quantile(n, m) + y[0], -10.f), 0.f);
   st->quantile = lq >= -0.02f ? 1.0f : exp2f(lq);
   // output 1: log2 of the degree split, in [1, 6]
   const int ls = (int)lrintf(fminf(fmaxf(y[1], 1.f), 6.f));
@@ -321,7 +333,7 @@ int ecl_learned_prepare(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s, void
   const int grid = std::max(1, std::min(sms * 4, (g->nodes + 511) / 512));
   k_feat_degrees<<<grid, 512, 0, s>>>(g->nindex, g->nodes, (FeatAcc*)d_acc);
   k_feat_finish<<<1, 1024, 0, s>>>(g->eweight, g->nodes, g->edges, (const FeatAcc*)d_acc, d_feat);
-  k_mlp_apply<<<1, 32, 0, s>>>(d_params, d_feat, (ecl::DevState*)st);
+  k_mlp_apply<<<1, 32, 0, s>>>(d_params, d_feat, g->nodes, g->edges, (ecl::DevState*)st);
   ML_TRY(cudaGetLastError());
   return ECL_OK;
 }
