@@ -21,6 +21,7 @@ using namespace ecl;
 namespace {
 constexpr int kDefaultSplit = 8;
 constexpr unsigned kDefaultSmallTail = 4096;
+constexpr int kLearnedMinEdges = 1 << 20;
 }  // namespace
 
 // =================================================================== host
@@ -47,10 +48,13 @@ struct ecl_mst_ctx {
   int* d_eweight = nullptr;
   unsigned char* d_inMST = nullptr;
   cudaEvent_t ev[5] = {};
-  // learned schedule: MLP parameters, the 16 features, degree accumulators
+  // learned schedule: MLP parameters (and the load they came from), the 16
+  // features, degree accumulators, the sorted 4096-entry weight sample
   float* ml_params = nullptr;
+  unsigned ml_version = ~0u;
   float* ml_feat = nullptr;
   void* ml_acc = nullptr;
+  int* ml_sample = nullptr;
 };
 
 namespace {
@@ -133,6 +137,7 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   if ((st = cuda_status(cudaMalloc(&c->ml_params, ECL_MLP_PARAMS * sizeof(float))))) return fail(st);
   if ((st = cuda_status(cudaMalloc(&c->ml_feat, ECL_MLP_INPUTS * sizeof(float))))) return fail(st);
   if ((st = cuda_status(cudaMalloc(&c->ml_acc, 64)))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->ml_sample, 4096 * sizeof(int))))) return fail(st);
   if ((st = cuda_status(cudaHostAlloc(&c->st_host, sizeof(DevState), cudaHostAllocDefault))))
     return fail(st);
   for (auto& e : c->ev)
@@ -154,6 +159,7 @@ extern "C" void ecl_mst_ctx_destroy(ecl_mst_ctx* c) {
   cudaFree(c->ml_params);
   cudaFree(c->ml_feat);
   cudaFree(c->ml_acc);
+  cudaFree(c->ml_sample);
   cudaFree(c->st);
   cudaFreeHost(c->st_host);
   cudaFree(c->d_nindex);
@@ -343,7 +349,10 @@ int check_opts(const mst_opts* o) {
 // trained MLP, writing DevState::quantile and DevState::learned_split.
 int ecl_learned_prepare(ecl_mst_ctx* c, const ecl_graph* d_graph, cudaStream_t s, void* st);
 
-int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, float** feat, void** acc, int* sm_count) {
+int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, float** feat, void** acc, int** sample,
+                            unsigned** version, int* sm_count) {
+  *sample = c->ml_sample;
+  *version = &c->ml_version;
   *params = c->ml_params;
   *feat = c->ml_feat;
   *acc = c->ml_acc;
@@ -369,6 +378,10 @@ extern "C" int ecl_mst_run_device(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d
     return ECL_OK;
   }
   ECL_CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevState), s));
+  // Graphs below kLearnedMinEdges CSR entries keep the reference heuristic:
+  // there the feature pass costs about as much as any schedule can save.
+  if (o.threshold_mode == ECL_THRESH_LEARNED && g->edges < kLearnedMinEdges)
+    o.threshold_mode = ECL_THRESH_HEURISTIC;
   if (o.threshold_mode == ECL_THRESH_LEARNED) {
     st = ecl_learned_prepare(c, g, s, c->st);
     if (st == ECL_ERR_UNSUPPORTED) o.threshold_mode = ECL_THRESH_HEURISTIC;  // no weights loaded

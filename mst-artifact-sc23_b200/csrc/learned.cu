@@ -101,8 +101,10 @@ __global__ void k_feat_degrees(const int* nindex, int n, FeatAcc* acc) {
 }
 
 // The 16 features, from the degree statistics and a sorted 4096-entry weight
-// sample (one CTA of 1024 threads).
-__global__ void k_feat_finish(const int* eweight, int n, int m, const FeatAcc* acc, float* out) {
+// sample (one CTA of 1024 threads). The sorted sample is also stored in
+// sorted_out (when not null) so the learned threshold can be read from it.
+__global__ void k_feat_finish(const int* eweight, int n, int m, const FeatAcc* acc, float* out,
+                              int* sorted_out) {
   __shared__ int samp[kSample];
   for (int i = threadIdx.x; i < kSample; i += blockDim.x) {
     const uint64_t r = ecl_mix64(0xFEA70000ull + (uint64_t)i);
@@ -123,6 +125,8 @@ __global__ void k_feat_finish(const int* eweight, int n, int m, const FeatAcc* a
       }
       __syncthreads();
     }
+  if (sorted_out)
+    for (int i = threadIdx.x; i < kSample; i += blockDim.x) sorted_out[i] = samp[i];
   if (threadIdx.x != 0) return;
   const double dn = (double)n, dm = (double)m;
   const double mean = dm / dn;
@@ -185,17 +189,49 @@ __host__ __device__ __forceinline__ float heuristic_log2_quantile(int n, int m) 
 // Decode the network output into the solve's control block. Output 0 is the
 // log2 quantile relative to the reference heuristic's; output 1 the log2
 // degree split.
-__global__ void k_mlp_apply(const float* p, const float* feat, int n, int m, ecl::DevState* st) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  float xs[kIn], h1[kH], h2[kH], y[kOut];
-  for (int i = 0; i < kIn; i++) xs[i] = (feat[i] - p[kOffMean + i]) / p[kOffStd + i];
-  mlp_forward1(p, xs, h1, h2, y);
-  // >= -0.02 means "no filter"
+// One CTA of kH threads: thread j computes hidden unit j of each layer. The
+// decoded quantile selects the light-phase threshold from the sorted weight
+// sample of the feature pass.
+__global__ void k_mlp_apply(const float* p, const float* feat, const int* sorted, int n, int m,
+                            ecl::DevState* st) {
+  __shared__ float xs[kIn], h1[kH], h2[kH], y[kOut];
+  const int j = threadIdx.x;
+  if (j < kIn) xs[j] = (feat[j] - p[kOffMean + j]) / p[kOffStd + j];
+  __syncthreads();
+  if (j < kH) {
+    float a = p[kOffB1 + j];
+    for (int i = 0; i < kIn; i++) a += xs[i] * p[kOffW1 + i * kH + j];
+    h1[j] = relu(a);
+  }
+  __syncthreads();
+  if (j < kH) {
+    float a = p[kOffB2 + j];
+    for (int i = 0; i < kH; i++) a += h1[i] * p[kOffW2 + i * kH + j];
+    h2[j] = relu(a);
+  }
+  __syncthreads();
+  if (j < kOut) {
+    float a = p[kOffB3 + j];
+    for (int i = 0; i < kH; i++) a += h2[i] * p[kOffW3 + i * kOut + j];
+    y[j] = a;
+  }
+  __syncthreads();
+  if (j != 0) return;
+  // output 0 (+ the heuristic's log2 quantile) >= -0.02 means "no filter"
   const float lq = fminf(fmaxf(heuristic_log2_quantile(n, m) + y[0], -10.f), 0.f);
-  st->quantile = lq >= -0.02f ? 1.0f : exp2f(lq);
+  const float q = lq >= -0.02f ? 1.0f : exp2f(lq);
+  st->quantile = q;
+  if (q < 1.0f) {
+    int idx = (int)(q * (float)(kSample - 1));
+    idx = idx < 0 ? 0 : (idx > kSample - 1 ? kSample - 1 : idx);
+    st->filtered = 1;
+    st->threshold = sorted[idx];
+  } else {
+    st->filtered = 0;
+    st->threshold = 0x7fffffff;
+  }
   // output 1: log2 of the degree split, in [1, 6]
-  const int ls = (int)lrintf(fminf(fmaxf(y[1], 1.f), 6.f));
-  st->learned_split = 1 << ls;
+  st->learned_split = 1 << (int)lrintf(fminf(fmaxf(y[1], 1.f), 6.f));
 }
 
 // Full-batch mean-squared-error loss and gradient of the trainable
@@ -292,11 +328,13 @@ __global__ void k_mlp_train(float* p, float* m1, float* m2, const float* x, cons
 
 std::mutex g_w_mu;
 std::vector<float> g_weights;  // host copy of the loaded parameter blob
+unsigned g_w_version = 0;      // bumped by every load; contexts re-upload on change
 
 }  // namespace
 
 struct ecl_mst_ctx;
-int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, float** feat, void** acc, int* sm_count);
+int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, float** feat, void** acc, int** sample,
+                            unsigned** version, int* sm_count);
 
 extern "C" int ecl_learned_set_weights(const float* params, int count) {
   if (count != kParams || !params) return ECL_ERR_INVALID_ARG;
@@ -304,6 +342,7 @@ extern "C" int ecl_learned_set_weights(const float* params, int count) {
     if (!(params[kOffStd + i] > 0.f)) return ECL_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lock(g_w_mu);
   g_weights.assign(params, params + count);
+  g_w_version++;
   return ECL_OK;
 }
 
@@ -317,23 +356,27 @@ extern "C" int ecl_learned_has_weights(void) {
 // ECL_ERR_UNSUPPORTED when no weights are loaded (the caller then falls back
 // to the reference heuristic).
 int ecl_learned_prepare(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s, void* st) {
-  std::vector<float> w;
-  {
-    std::lock_guard<std::mutex> lock(g_w_mu);
-    w = g_weights;
-  }
-  if (w.empty()) return ECL_ERR_UNSUPPORTED;
   float *d_params, *d_feat;
   void* d_acc;
+  int* d_sample;
+  unsigned* version;
   int sms = 0;
-  int r = ecl_ctx_learned_buffers(c, &d_params, &d_feat, &d_acc, &sms);
+  int r = ecl_ctx_learned_buffers(c, &d_params, &d_feat, &d_acc, &d_sample, &version, &sms);
   if (r) return r;
-  ML_TRY(cudaMemcpyAsync(d_params, w.data(), kParams * sizeof(float), cudaMemcpyHostToDevice, s));
+  {
+    std::lock_guard<std::mutex> lock(g_w_mu);
+    if (g_weights.empty()) return ECL_ERR_UNSUPPORTED;
+    if (*version != g_w_version) {  // upload only when the loaded weights changed
+      ML_TRY(cudaMemcpyAsync(d_params, g_weights.data(), kParams * sizeof(float), cudaMemcpyHostToDevice, s));
+      ML_TRY(cudaStreamSynchronize(s));
+      *version = g_w_version;
+    }
+  }
   ML_TRY(cudaMemsetAsync(d_acc, 0, sizeof(FeatAcc), s));
   const int grid = std::max(1, std::min(sms * 4, (g->nodes + 511) / 512));
   k_feat_degrees<<<grid, 512, 0, s>>>(g->nindex, g->nodes, (FeatAcc*)d_acc);
-  k_feat_finish<<<1, 1024, 0, s>>>(g->eweight, g->nodes, g->edges, (const FeatAcc*)d_acc, d_feat);
-  k_mlp_apply<<<1, 32, 0, s>>>(d_params, d_feat, g->nodes, g->edges, (ecl::DevState*)st);
+  k_feat_finish<<<1, 1024, 0, s>>>(g->eweight, g->nodes, g->edges, (const FeatAcc*)d_acc, d_feat, d_sample);
+  k_mlp_apply<<<1, kH, 0, s>>>(d_params, d_feat, d_sample, g->nodes, g->edges, (ecl::DevState*)st);
   ML_TRY(cudaGetLastError());
   return ECL_OK;
 }
@@ -355,7 +398,7 @@ extern "C" int ecl_graph_features(const ecl_graph* g, float* out) {
   cudaMemset(acc, 0, sizeof(FeatAcc));
   const int grid = std::max(1, std::min(sms * 4, (g->nodes + 511) / 512));
   k_feat_degrees<<<grid, 512>>>(g->nindex, g->nodes, acc);
-  k_feat_finish<<<1, 1024>>>(g->eweight, g->nodes, g->edges, acc, f);
+  k_feat_finish<<<1, 1024>>>(g->eweight, g->nodes, g->edges, acc, f, nullptr);
   cudaError_t e = cudaMemcpy(out, f, kIn * sizeof(float), cudaMemcpyDeviceToHost);
   cudaFree(acc);
   cudaFree(f);

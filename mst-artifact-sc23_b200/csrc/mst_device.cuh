@@ -107,16 +107,16 @@ struct RoundArgs {
 // ------------------------------------------------------------------ prep
 // Threshold rule, by mode (run by one CTA). HEURISTIC restates main's rule
 // (ECL_MST.cu:408,432-440); QUANTILE takes a quantile of a 4096-entry hashed
-// sample; LEARNED reads the quantile and split the MLP wrote into `st`.
+// sample; LEARNED keeps the threshold, filter flag and split the MLP kernel
+// already wrote into `st` (from its own sorted sample).
 __device__ void choose_threshold(const PrepArgs& a, int* samp) {
   DevState* st = a.st;
   const int tid = threadIdx.x;
   int mode = a.mode, split = a.split;
   float quantile = a.quantile;
   if (mode == ECL_THRESH_LEARNED) {
-    quantile = st->quantile;
-    split = st->learned_split;
-    mode = ECL_THRESH_QUANTILE;
+    if (tid == 0) st->split = st->learned_split;
+    return;
   }
   const int nodes = a.nodes, edges = a.edges;
   if (tid == 0) st->split = split;
