@@ -267,7 +267,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat22")
-    ap.add_argument("--mode", choices=["heuristic", "learned", "quantile"], default="heuristic")
+    ap.add_argument("--mode", choices=["heuristic", "learned", "quantile"], default="learned")
     ap.add_argument("--quantile", type=float, default=0.1)
     ap.add_argument("--split", type=int, default=0)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain ECL-MST comparison")
@@ -302,6 +302,9 @@ def main():
     g = make_graph(E, kind, kw)
     gen_s = time.perf_counter() - t0
 
+    have_weights = E.learned_load_default()
+    if args.mode == "learned" and not have_weights:
+        args.mode = "heuristic"  # the reference heuristic is the learned schedule's fallback
     mode = {"heuristic": E.THRESH_HEURISTIC, "learned": E.THRESH_LEARNED, "quantile": E.THRESH_QUANTILE}[args.mode]
     opts = E.make_opts(mode=mode, quantile=args.quantile, degree_split=args.split)
 
@@ -347,6 +350,17 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_step = float(t.item())
     value = world * g.edges / (ms_step * 1e-3) / 1e9
+
+    # the same solve under the reference heuristic's schedule, for comparison
+    heur_ms = []
+    if args.mode != "heuristic":
+        for i in range(args.warmup + max(3, args.steps // 2)):
+            flush.zero_()
+            st_h = ctx.run_device(g.nodes, g.edges, d_ni.data_ptr(), d_nl.data_ptr(), d_ew.data_ptr(),
+                                  d_out.data_ptr(), opts=E.make_opts(degree_split=args.split),
+                                  stream=stream.cuda_stream, stats=True)
+            if i >= args.warmup:
+                heur_ms.append(st_h["ms_total"])
 
     # one extra solve counting the guarded atomics for the byte model
     st_atom = ctx.run_device(g.nodes, g.edges, d_ni.data_ptr(), d_nl.data_ptr(), d_ew.data_ptr(),
@@ -456,7 +470,13 @@ def main():
                        "ms_median": statistics.median(step_ms), "gen_s": round(gen_s, 2)},
             "e2e": {"value": world * g.edges / e2e_mean / 1e9, "unit": "Gedges/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms": e2e_mean * 1e3},
-            "gpu_launches": 5 * args.steps,
+            # per solve: k_prep, k_scan x2, k_rounds x2, k_flatten; the learned schedule adds
+            # k_feat_degrees, k_feat_finish, k_mlp_apply and launches all three scan variants
+            "gpu_launches": (13 if args.mode == "learned" else 6) * args.steps,
+            "heuristic_schedule": ({"value": world * g.edges / (np.mean(heur_ms) * 1e-3) / 1e9,
+                                    "ms": float(np.mean(heur_ms)),
+                                    "what": "same solve with the reference threshold heuristic"}
+                                   if heur_ms else None),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "plain_ecl_mst": plain,
