@@ -87,6 +87,8 @@ int coop_grid(const void* fn, int threads, int sm_count) {
   return per_sm * sm_count;
 }
 
+int prepare_scan_kernels();
+
 }  // namespace
 
 extern "C" void ecl_default_opts(mst_opts* o) {
@@ -143,6 +145,7 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   for (auto& e : c->ev)
     if ((st = cuda_status(cudaEventCreate(&e)))) return fail(st);
   c->round_grid = coop_grid((const void*)k_rounds, kThreads, c->sm_count);
+  if ((st = prepare_scan_kernels())) return fail(st);
   if (c->round_grid <= 0) return fail(ECL_ERR_CUDA);
   *out = c;
   return ECL_OK;
@@ -190,13 +193,27 @@ int launch_coop(const void* fn, int grid, int threads, void* arg, cudaStream_t s
   return cuda_status(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, 0, s));
 }
 
+// Opt the scan variants into their dynamic shared memory (once per device).
+int prepare_scan_kernels() {
+  ECL_CUDA_TRY(cudaFuncSetAttribute(k_scan<kLight, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scan_smem_bytes<4>()));
+  ECL_CUDA_TRY(cudaFuncSetAttribute(k_scan<kLight, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scan_smem_bytes<8>()));
+  ECL_CUDA_TRY(cudaFuncSetAttribute(k_scan<kLight, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scan_smem_bytes<16>()));
+  ECL_CUDA_TRY(cudaFuncSetAttribute(k_scan<kHeavy, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scan_smem_bytes<4>()));
+  ECL_CUDA_TRY(cudaFuncSetAttribute(k_scan<kHeavy, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scan_smem_bytes<8>()));
+  ECL_CUDA_TRY(cudaFuncSetAttribute(k_scan<kHeavy, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scan_smem_bytes<16>()));
+  return ECL_OK;
+}
+
+// Persistent scan: one CTA per resident slot (at most grid_cap), each
+// looping over tiles.
 template <int KIND>
 int launch_scan(int ept, const ScanArgs& sa, cudaStream_t s) {
   const int m = sa.edges;
-  const int blocks = (int)((m + (int64_t)kScanThreads * ept - 1) / ((int64_t)kScanThreads * ept));
-  if (ept == 4) k_scan<KIND, 4><<<blocks, kScanThreads, 0, s>>>(sa);
-  else if (ept == 8) k_scan<KIND, 8><<<blocks, kScanThreads, 0, s>>>(sa);
-  else k_scan<KIND, 16><<<blocks, kScanThreads, 0, s>>>(sa);
+  const int tiles = (int)((m + (int64_t)kScanThreads * ept - 1) / ((int64_t)kScanThreads * ept));
+  const int blocks = std::max(1, std::min(tiles, sa.grid_cap));
+  if (ept == 4) k_scan<KIND, 4><<<blocks, kScanThreads, scan_smem_bytes<4>(), s>>>(sa);
+  else if (ept == 8) k_scan<KIND, 8><<<blocks, kScanThreads, scan_smem_bytes<8>(), s>>>(sa);
+  else k_scan<KIND, 16><<<blocks, kScanThreads, scan_smem_bytes<16>(), s>>>(sa);
   return cuda_status(cudaGetLastError());
 }
 
@@ -252,6 +269,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   sa.vec_ok = ((((uintptr_t)g->nlist) | ((uintptr_t)g->eweight)) & 15) == 0;
   sa.zero_vec = (((uintptr_t)d_inMST) & 15) == 0;
   sa.st = c->st;
+  sa.grid_cap = c->sm_count * 4;
   RoundArgs ra;
   ra.nodes = n;
   ra.wl0 = c->wl[0];
@@ -515,6 +533,8 @@ int na_setup(int dev, NaDevice** out) {
     if (!coop) return ECL_ERR_UNSUPPORTED;
     ECL_CUDA_TRY(cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev));
     d.round_grid = coop_grid((const void*)k_rounds, kThreads, d.sm_count);
+    int ps = prepare_scan_kernels();
+    if (ps) return ps;
     if (d.round_grid <= 0) return ECL_ERR_CUDA;
     d.base = (unsigned char*)p;
     d.ready = true;
@@ -590,6 +610,7 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   sa.vec_ok = ((((uintptr_t)g->nlist) | ((uintptr_t)g->eweight)) & 15) == 0;
   sa.zero_vec = (((uintptr_t)d_inMST) & 15) == 0;
   sa.st = dst;
+  sa.grid_cap = d->sm_count * 4;
   RoundArgs ra;
   ra.nodes = n;
   ra.wl0 = wl0;

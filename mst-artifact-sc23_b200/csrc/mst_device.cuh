@@ -23,6 +23,7 @@
 //   k_scan<H,E>   initWL<false>: keeps heavy entries across light trees
 //   k_rounds      heavy phase
 #pragma once
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 #include <climits>
 #include <stdint.h>
@@ -86,6 +87,7 @@ struct ScanArgs {
   unsigned char* inMST;
   int vec_ok;    // nlist / eweight 16-byte aligned
   int zero_vec;  // inMST 16-byte aligned
+  int grid_cap;  // host side: CTAs of the persistent scan launch
   DevState* st;
 };
 
@@ -236,9 +238,52 @@ enum ScanKind { kLight = 0, kHeavy = 1 };
 // are appended as {rep(v), rep(n), w, j}; the heavy scan additionally drops
 // entries whose endpoints share a light-phase tree (parent[] is flat, so a
 // rep is one load).
+// Asynchronous global -> shared copies (cp.async) of one tile: the thread's
+// own EPT entries of nlist and eweight (16-byte copies when aligned), and a
+// cooperative copy of the tile's nindex slice when it fits in shared memory.
+template <int EPT>
+__device__ __forceinline__ void scan_issue_tile(const ScanArgs& a, long long e0, int v_lo, int span,
+                                                int* nl_s, int* ew_s, int* sidx) {
+  const int m = a.edges;
+  const long long j0 = e0 + (long long)threadIdx.x * EPT;
+  int* nl_d = nl_s + threadIdx.x * EPT;
+  int* ew_d = ew_s + threadIdx.x * EPT;
+  if (a.vec_ok && j0 + EPT <= m) {
+#pragma unroll
+    for (int q = 0; q < EPT; q += 4) {
+      __pipeline_memcpy_async(nl_d + q, a.nlist + j0 + q, 16);
+      __pipeline_memcpy_async(ew_d + q, a.eweight + j0 + q, 16);
+    }
+  } else {
+    for (int q = 0; q < EPT && j0 + q < m; q++) {
+      __pipeline_memcpy_async(nl_d + q, a.nlist + j0 + q, 4);
+      __pipeline_memcpy_async(ew_d + q, a.eweight + j0 + q, 4);
+    }
+  }
+  if (span <= kSegCap)
+    for (int i = threadIdx.x; i <= span; i += blockDim.x) __pipeline_memcpy_async(sidx + i, a.nindex + v_lo + i, 4);
+  __pipeline_commit();
+}
+
+// Persistent, double-buffered: while a CTA decides its current tile from
+// shared memory, the next tile's entries and nindex slice are already on
+// their way (cp.async), and the first_v pair of the tile after that is in
+// registers, so the only serial latency per tile is the reservation.
+// Dynamic shared memory of a scan CTA: two stages of (nlist, eweight) tiles
+// and two nindex slices.
+template <int EPT>
+constexpr size_t scan_smem_bytes() {
+  return 2 * 2 * (size_t)kScanThreads * EPT * sizeof(int) + 2 * (size_t)(kSegCap + 4) * sizeof(int);
+}
+
 template <int KIND, int EPT>
-__global__ void __launch_bounds__(kScanThreads, EPT == 16 ? 2 : 4) k_scan(ScanArgs a) {
-  __shared__ int sidx[kSegCap + 1];
+__global__ void __launch_bounds__(kScanThreads, EPT == 16 ? 2 : 3) k_scan(ScanArgs a) {
+  constexpr int kTile = kScanThreads * EPT;
+  constexpr int kStep = EPT / 4;  // first_v entries per tile
+  extern __shared__ __align__(16) int scan_dyn[];
+  int (*nl_s)[kTile] = reinterpret_cast<int (*)[kTile]>(scan_dyn);
+  int (*ew_s)[kTile] = reinterpret_cast<int (*)[kTile]>(scan_dyn + 2 * kTile);
+  int (*sidx_s)[kSegCap + 4] = reinterpret_cast<int (*)[kSegCap + 4]>(scan_dyn + 4 * kTile);
   __shared__ ReserveSmem sm;
   DevState* st = a.st;
   if (ld_volatile(&st->error) & kErrFormat) return;  // set by k_prep only
@@ -246,40 +291,41 @@ __global__ void __launch_bounds__(kScanThreads, EPT == 16 ? 2 : 4) k_scan(ScanAr
   if (scan_ept(st->split) != EPT) return;  // only the variant the split selects runs
   const int thr = st->threshold;
   const int n = a.nodes, m = a.edges;
-  constexpr int kTile = kScanThreads * EPT;
-  constexpr int kStep = EPT / 4;  // first_v entries per tile
-  const long long e0 = (long long)blockIdx.x * kTile;
-  if (e0 >= m) return;
-  const long long j0 = e0 + (long long)threadIdx.x * EPT;
-  // The tile's CSR loads go out first; the vertex lookup below overlaps them.
-  int nb[EPT], w[EPT];
-  if (j0 + EPT <= m && a.vec_ok) {
-#pragma unroll
-    for (int q = 0; q < EPT; q += 4) {
-      const int4 x = __ldg(reinterpret_cast<const int4*>(a.nlist + j0 + q));
-      const int4 y = __ldg(reinterpret_cast<const int4*>(a.eweight + j0 + q));
-      nb[q] = x.x; nb[q + 1] = x.y; nb[q + 2] = x.z; nb[q + 3] = x.w;
-      w[q] = y.x; w[q + 1] = y.y; w[q + 2] = y.z; w[q + 3] = y.w;
-    }
-  } else {
+  const int ntiles = (int)(((long long)m + kTile - 1) / kTile);
+  int t = blockIdx.x;
+  if (t >= ntiles) return;
+  const int stride = gridDim.x;
+  auto first_v = [&](int tile) -> int2 {
+    const int tb = tile * kStep;
+    return make_int2(__ldg(a.first_v + tb), __ldg(a.first_v + min(tb + kStep, a.tiles)));
+  };
+  int2 fv_cur = first_v(t);
+  int2 fv_nxt = t + stride < ntiles ? first_v(t + stride) : make_int2(0, 0);
+  scan_issue_tile<EPT>(a, (long long)t * kTile, fv_cur.x, fv_cur.y - fv_cur.x + 1, nl_s[0], ew_s[0], sidx_s[0]);
+  __pipeline_wait_prior(0);
+  __syncthreads();
+  for (int buf = 0; t < ntiles; t += stride, buf ^= 1) {
+    const int tn = t + stride;
+    if (tn < ntiles)
+      scan_issue_tile<EPT>(a, (long long)tn * kTile, fv_nxt.x, fv_nxt.y - fv_nxt.x + 1, nl_s[buf ^ 1],
+                           ew_s[buf ^ 1], sidx_s[buf ^ 1]);
+    const int2 fv_after = tn + stride < ntiles ? first_v(tn + stride) : make_int2(0, 0);
+    const long long e0 = (long long)t * kTile;
+    const long long j0 = e0 + (long long)threadIdx.x * EPT;
+    const int v_lo = fv_cur.x;
+    const int span = fv_cur.y - fv_cur.x + 1;  // vertices whose rows may hold this tile's entries
+    const bool seg = span <= kSegCap;
+    const int* sidx = sidx_s[buf];
+    auto row_start = [&](int i) -> int {  // nindex[v_lo + i]
+      return seg ? sidx[i] : __ldg(a.nindex + v_lo + i);
+    };
+    int nb[EPT], w[EPT];
 #pragma unroll
     for (int q = 0; q < EPT; q++) {
       const bool in = j0 + q < m;
-      nb[q] = in ? __ldg(a.nlist + j0 + q) : -1;
-      w[q] = in ? __ldg(a.eweight + j0 + q) : 0;
+      nb[q] = in ? nl_s[buf][threadIdx.x * EPT + q] : -1;
+      w[q] = in ? ew_s[buf][threadIdx.x * EPT + q] : 0;
     }
-  }
-  const int tb = blockIdx.x * kStep;
-  const int v_lo = __ldg(a.first_v + tb);
-  const int v_hi = __ldg(a.first_v + min(tb + kStep, a.tiles));
-  const int span = v_hi - v_lo + 1;  // vertices whose rows may hold this tile's entries
-  const bool seg = span <= kSegCap;
-  if (seg)
-    for (int i = threadIdx.x; i <= span; i += blockDim.x) sidx[i] = __ldg(a.nindex + v_lo + i);
-  __syncthreads();
-  auto row_start = [&](int i) -> int {  // nindex[v_lo + i]
-    return seg ? sidx[i] : __ldg(a.nindex + v_lo + i);
-  };
   if (KIND == kLight && j0 < m) {  // inMST = 0 (the reference memsets it, :306)
     if (a.zero_vec && j0 + EPT <= m) {
       if (EPT == 4) *reinterpret_cast<unsigned*>(a.inMST + j0) = 0u;
@@ -343,6 +389,12 @@ __global__ void __launch_bounds__(kScanThreads, EPT == 16 ? 2 : 4) k_scan(ScanAr
     if (pos < a.wl_cap) a.wl[pos] = make_int4(vtx[q], nrep[q], w[q], (int)(j0 + q));
     else atomicOr(&st->error, kErrOverflow);
     pos++;
+  }
+    // the next tile's copies must have landed (all threads') before it is read
+    __pipeline_wait_prior(0);
+    __syncthreads();
+    fv_cur = fv_nxt;
+    fv_nxt = fv_after;
   }
 }
 
