@@ -204,17 +204,25 @@ int prepare_scan_kernels() {
   return ECL_OK;
 }
 
-// Persistent scan: one CTA per resident slot (at most grid_cap), each
-// looping over tiles.
+// Persistent scan: exactly as many CTAs as can be resident at once (a CTA
+// started late would finish its share late), each looping over tiles.
+template <int KIND, int EPT>
+int launch_scan_ept(const ScanArgs& sa, cudaStream_t s) {
+  const int m = sa.edges;
+  const int tiles = (int)((m + (int64_t)kScanThreads * EPT - 1) / ((int64_t)kScanThreads * EPT));
+  int per_sm = 0;
+  ECL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan<KIND, EPT>, kScanThreads,
+                                                             scan_smem_bytes<EPT>()));
+  const int blocks = std::max(1, std::min(tiles, std::max(1, per_sm) * sa.sm_count));
+  k_scan<KIND, EPT><<<blocks, kScanThreads, scan_smem_bytes<EPT>(), s>>>(sa);
+  return cuda_status(cudaGetLastError());
+}
+
 template <int KIND>
 int launch_scan(int ept, const ScanArgs& sa, cudaStream_t s) {
-  const int m = sa.edges;
-  const int tiles = (int)((m + (int64_t)kScanThreads * ept - 1) / ((int64_t)kScanThreads * ept));
-  const int blocks = std::max(1, std::min(tiles, sa.grid_cap));
-  if (ept == 4) k_scan<KIND, 4><<<blocks, kScanThreads, scan_smem_bytes<4>(), s>>>(sa);
-  else if (ept == 8) k_scan<KIND, 8><<<blocks, kScanThreads, scan_smem_bytes<8>(), s>>>(sa);
-  else k_scan<KIND, 16><<<blocks, kScanThreads, scan_smem_bytes<16>(), s>>>(sa);
-  return cuda_status(cudaGetLastError());
+  if (ept == 4) return launch_scan_ept<KIND, 4>(sa, s);
+  if (ept == 8) return launch_scan_ept<KIND, 8>(sa, s);
+  return launch_scan_ept<KIND, 16>(sa, s);
 }
 
 // Scan variants to launch: the one the split selects, or all three (each
@@ -269,7 +277,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   sa.vec_ok = ((((uintptr_t)g->nlist) | ((uintptr_t)g->eweight)) & 15) == 0;
   sa.zero_vec = (((uintptr_t)d_inMST) & 15) == 0;
   sa.st = c->st;
-  sa.grid_cap = c->sm_count * 4;
+  sa.sm_count = c->sm_count;
   RoundArgs ra;
   ra.nodes = n;
   ra.wl0 = c->wl[0];
@@ -610,7 +618,7 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   sa.vec_ok = ((((uintptr_t)g->nlist) | ((uintptr_t)g->eweight)) & 15) == 0;
   sa.zero_vec = (((uintptr_t)d_inMST) & 15) == 0;
   sa.st = dst;
-  sa.grid_cap = d->sm_count * 4;
+  sa.sm_count = d->sm_count;
   RoundArgs ra;
   ra.nodes = n;
   ra.wl0 = wl0;

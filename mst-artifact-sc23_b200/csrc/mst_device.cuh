@@ -87,7 +87,7 @@ struct ScanArgs {
   unsigned char* inMST;
   int vec_ok;    // nlist / eweight 16-byte aligned
   int zero_vec;  // inMST 16-byte aligned
-  int grid_cap;  // host side: CTAs of the persistent scan launch
+  int sm_count;  // host side: sizes the persistent scan launch
   DevState* st;
 };
 
@@ -273,7 +273,8 @@ __device__ __forceinline__ void scan_issue_tile(const ScanArgs& a, long long e0,
 // and two nindex slices.
 template <int EPT>
 constexpr size_t scan_smem_bytes() {
-  return 2 * 2 * (size_t)kScanThreads * EPT * sizeof(int) + 2 * (size_t)(kSegCap + 4) * sizeof(int);
+  return 2 * 2 * (size_t)kScanThreads * EPT * sizeof(int) + 2 * (size_t)(kSegCap + 4) * sizeof(int) +
+         (size_t)kScanThreads * EPT * sizeof(int);
 }
 
 template <int KIND, int EPT>
@@ -284,13 +285,17 @@ __global__ void __launch_bounds__(kScanThreads, EPT == 16 ? 2 : 3) k_scan(ScanAr
   int (*nl_s)[kTile] = reinterpret_cast<int (*)[kTile]>(scan_dyn);
   int (*ew_s)[kTile] = reinterpret_cast<int (*)[kTile]>(scan_dyn + 2 * kTile);
   int (*sidx_s)[kSegCap + 4] = reinterpret_cast<int (*)[kSegCap + 4]>(scan_dyn + 4 * kTile);
-  __shared__ ReserveSmem sm;
+  // row-start marks of the current tile: (generation << 13) | (span index + 1)
+  int* rmark = scan_dyn + 4 * kTile + 2 * (kSegCap + 4);
+  __shared__ unsigned warp_off[kScanThreads / 32];
+  __shared__ unsigned tile_base;
   DevState* st = a.st;
   if (ld_volatile(&st->error) & kErrFormat) return;  // set by k_prep only
   if (KIND == kHeavy && !st->filtered) return;
   if (scan_ept(st->split) != EPT) return;  // only the variant the split selects runs
   const int thr = st->threshold;
   const int n = a.nodes, m = a.edges;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int ntiles = (int)(((long long)m + kTile - 1) / kTile);
   int t = blockIdx.x;
   if (t >= ntiles) return;
@@ -302,6 +307,8 @@ __global__ void __launch_bounds__(kScanThreads, EPT == 16 ? 2 : 3) k_scan(ScanAr
   int2 fv_cur = first_v(t);
   int2 fv_nxt = t + stride < ntiles ? first_v(t + stride) : make_int2(0, 0);
   scan_issue_tile<EPT>(a, (long long)t * kTile, fv_cur.x, fv_cur.y - fv_cur.x + 1, nl_s[0], ew_s[0], sidx_s[0]);
+  for (int q = threadIdx.x; q < kTile; q += blockDim.x) rmark[q] = 0;  // generation 0 never matches
+  int gen = 0;
   __pipeline_wait_prior(0);
   __syncthreads();
   for (int buf = 0; t < ntiles; t += stride, buf ^= 1) {
@@ -319,80 +326,138 @@ __global__ void __launch_bounds__(kScanThreads, EPT == 16 ? 2 : 3) k_scan(ScanAr
     auto row_start = [&](int i) -> int {  // nindex[v_lo + i]
       return seg ? sidx[i] : __ldg(a.nindex + v_lo + i);
     };
+    // the thread's own entries, 128 bits at a time from the staged tile
     int nb[EPT], w[EPT];
+    if (j0 + EPT <= m) {
+#pragma unroll
+      for (int q = 0; q < EPT; q += 4) {
+        const int4 x = *reinterpret_cast<const int4*>(&nl_s[buf][threadIdx.x * EPT + q]);
+        const int4 y = *reinterpret_cast<const int4*>(&ew_s[buf][threadIdx.x * EPT + q]);
+        nb[q] = x.x; nb[q + 1] = x.y; nb[q + 2] = x.z; nb[q + 3] = x.w;
+        w[q] = y.x; w[q + 1] = y.y; w[q + 2] = y.z; w[q + 3] = y.w;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < EPT; q++) {
+        const bool in = j0 + q < m;
+        nb[q] = in ? nl_s[buf][threadIdx.x * EPT + q] : -1;
+        w[q] = in ? ew_s[buf][threadIdx.x * EPT + q] : 0;
+      }
+    }
+    if (KIND == kLight && j0 < m) {  // inMST = 0 (the reference memsets it, :306)
+      if (a.zero_vec && j0 + EPT <= m) {
+        if (EPT == 4) *reinterpret_cast<unsigned*>(a.inMST + j0) = 0u;
+        else if (EPT == 8) *reinterpret_cast<uint2*>(a.inMST + j0) = make_uint2(0u, 0u);
+        else *reinterpret_cast<uint4*>(a.inMST + j0) = make_uint4(0u, 0u, 0u, 0u);
+      } else {
+        for (int q = 0; q < EPT && j0 + q < m; q++) a.inMST[j0 + q] = 0;
+      }
+    }
+    // Vertex of every entry without a per-entry walk: each row starting
+    // inside the tile marks its start position with its span index (the
+    // largest index wins, so a run of zero-degree rows resolves to the row
+    // that owns the entries); an entry's vertex is then the largest mark at
+    // or before it, seeded with the vertex of the thread's first entry.
+    // (Tiles whose vertex range exceeds the shared slice, i.e. long runs of
+    // zero-degree vertices, search each entry in global nindex instead.)
+    auto last_row_at_or_before = [&](long long j) -> int {
+      int lo = 0, hi = span;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (row_start(mid) <= j) lo = mid;
+        else hi = mid;
+      }
+      return lo;
+    };
+    gen++;
+    if (seg)
+      for (int r = 1 + threadIdx.x; r < span; r += blockDim.x) {
+        const long long p = (long long)sidx[r] - e0;
+        if (p > 0 && p < kTile) atomicMax(&rmark[p], (gen << 13) | (r + 1));
+      }
+    const int i0 = j0 < m ? last_row_at_or_before(j0) : 0;  // vertex of entry j0
+    __syncthreads();
+    int vi[EPT];
+    if (seg) {
+      int run = i0;
+#pragma unroll
+      for (int q = 0; q < EPT; q += 4) {
+        const int4 mk = *reinterpret_cast<const int4*>(&rmark[threadIdx.x * EPT + q]);
+        const int c[4] = {mk.x, mk.y, mk.z, mk.w};
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          if ((c[u] >> 13) == gen) run = max(run, (c[u] & 8191) - 1);
+          vi[q + u] = run;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < EPT; q++) vi[q] = j0 + q < m ? last_row_at_or_before(j0 + q) : 0;
+    }
+    int vtx[EPT], nrep[EPT];
+    unsigned keep = 0, cnt = 0;
+    int cur_v = -1, cur_rep = -1;
 #pragma unroll
     for (int q = 0; q < EPT; q++) {
-      const bool in = j0 + q < m;
-      nb[q] = in ? nl_s[buf][threadIdx.x * EPT + q] : -1;
-      w[q] = in ? ew_s[buf][threadIdx.x * EPT + q] : 0;
-    }
-  if (KIND == kLight && j0 < m) {  // inMST = 0 (the reference memsets it, :306)
-    if (a.zero_vec && j0 + EPT <= m) {
-      if (EPT == 4) *reinterpret_cast<unsigned*>(a.inMST + j0) = 0u;
-      else if (EPT == 8) *reinterpret_cast<uint2*>(a.inMST + j0) = make_uint2(0u, 0u);
-      else *reinterpret_cast<uint4*>(a.inMST + j0) = make_uint4(0u, 0u, 0u, 0u);
-    } else {
-      for (int q = 0; q < EPT && j0 + q < m; q++) a.inMST[j0 + q] = 0;
-    }
-  }
-  // vertex of entry j0: the last i in [0, span) with row_start(i) <= j0
-  int i = 0;
-  if (j0 < m) {
-    int lo = 0, hi = span;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (row_start(mid) <= j0) lo = mid;
-      else hi = mid;
-    }
-    i = lo;
-  }
-  int row_end = row_start(i + 1);
-  int vtx[EPT], nrep[EPT];
-  unsigned keep = 0, cnt = 0;
-  int cur_v = -1, cur_rep = -1;
-#pragma unroll
-  for (int q = 0; q < EPT; q++) {
-    const long long j = j0 + q;
-    vtx[q] = 0;
-    nrep[q] = nb[q];
-    if (j >= m) continue;
-    while (j >= row_end && i < span - 1) {  // skip to the row holding j (zero-degree rows too)
-      i++;
-      row_end = row_start(i + 1);
-    }
-    const int v = v_lo + i;
-    if ((unsigned)nb[q] >= (unsigned)n) {
-      atomicOr(&st->error, kErrFormat);
-      continue;
-    }
-    if (nb[q] <= v) continue;
-    if (KIND == kLight ? !(w[q] <= thr) : !(w[q] > thr)) continue;
-    int rv = v;
-    if (KIND == kHeavy) {
-      if (v != cur_v) {
-        cur_v = v;
-        cur_rep = __ldg(a.parent + v);
+      const long long j = j0 + q;
+      vtx[q] = 0;
+      nrep[q] = nb[q];
+      if (j >= m) continue;
+      const int v = v_lo + vi[q];
+      if ((unsigned)nb[q] >= (unsigned)n) {
+        atomicOr(&st->error, kErrFormat);
+        continue;
       }
-      rv = cur_rep;
-      nrep[q] = __ldg(a.parent + nb[q]);
-      if (nrep[q] == rv) continue;
+      if (nb[q] <= v) continue;
+      if (KIND == kLight ? !(w[q] <= thr) : !(w[q] > thr)) continue;
+      int rv = v;
+      if (KIND == kHeavy) {
+        if (v != cur_v) {
+          cur_v = v;
+          cur_rep = __ldg(a.parent + v);
+        }
+        rv = cur_rep;
+        nrep[q] = __ldg(a.parent + nb[q]);
+        if (nrep[q] == rv) continue;
+      }
+      vtx[q] = rv;
+      keep |= 1u << q;
+      cnt++;
     }
-    vtx[q] = rv;
-    keep |= 1u << q;
-    cnt++;
-  }
-  unsigned pos, unused;
-  cta_reserve2(cnt, 0u, &st->wl_count[KIND][0], nullptr, sm, pos, unused);
+    // Tile reservation. Its two barriers double as the pipeline's: before
+    // the first, every thread has finished reading this tile's stage and has
+    // waited for its own copies of the next tile, so after it the next stage
+    // is complete and this one may be refilled.
+    unsigned incl = cnt;
 #pragma unroll
-  for (int q = 0; q < EPT; q++) {
-    if (!(keep & (1u << q))) continue;
-    if (pos < a.wl_cap) a.wl[pos] = make_int4(vtx[q], nrep[q], w[q], (int)(j0 + q));
-    else atomicOr(&st->error, kErrOverflow);
-    pos++;
-  }
-    // the next tile's copies must have landed (all threads') before it is read
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned x = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += x;
+    }
+    if (lane == 31) warp_off[warp] = incl;
     __pipeline_wait_prior(0);
     __syncthreads();
+    if (warp == 0) {
+      constexpr int nw = kScanThreads / 32;
+      const unsigned w0 = lane < nw ? warp_off[lane] : 0u;
+      unsigned x0 = w0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned x = __shfl_up_sync(0xffffffffu, x0, o);
+        if (lane >= o) x0 += x;
+      }
+      if (lane < nw) warp_off[lane] = x0 - w0;
+      if (lane == 31) tile_base = x0 ? atomicAdd(&st->wl_count[KIND][0], x0) : 0u;
+    }
+    __syncthreads();
+    unsigned pos = tile_base + warp_off[warp] + (incl - cnt);
+#pragma unroll
+    for (int q = 0; q < EPT; q++) {
+      if (!(keep & (1u << q))) continue;
+      if (pos < a.wl_cap) a.wl[pos] = make_int4(vtx[q], nrep[q], w[q], (int)(j0 + q));
+      else atomicOr(&st->error, kErrOverflow);
+      pos++;
+    }
     fv_cur = fv_nxt;
     fv_nxt = fv_after;
   }
