@@ -85,6 +85,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.skip = 0
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -95,6 +96,14 @@ class ClockSampler:
                  "-lms", "20"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
+            return self
+        # the timed region starts once the sampler is producing samples
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.01)
+        self.skip = sum(1 for _ in open(self.path))  # samples taken before the timed region
         return self
 
     def __exit__(self, *exc):
@@ -111,7 +120,9 @@ class ClockSampler:
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         with open(self.path) as f:
-            for line in f:
+            for k, line in enumerate(f):
+                if k < self.skip:
+                    continue
                 parts = [p.strip() for p in line.split(",")]
                 if len(parts) < 9:
                     continue
@@ -263,7 +274,7 @@ def reference_arm(args, E):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat22")

@@ -169,15 +169,18 @@ typedef struct ecl_mst_stats {
   int32_t rounds[2];       /* Boruvka rounds of the light / heavy phase         */
   int32_t status;          /* device error word (0 = clean)                     */
   int64_t scan_kept[2];    /* worklist entries appended by each scan            */
-  int64_t wl_in[2][ECL_MAX_ROUNDS];  /* worklist size entering each round      */
+  int64_t wl_in[2][ECL_MAX_ROUNDS];  /* worklist slots entering each round (the
+                                        first also holds null padding)       */
   int64_t atomics;         /* guarded atomicMin issued (ECL_FLAG_STATS only)    */
   int64_t forest_edges;    /* number of inMST entries set                       */
   uint64_t forest_weight;  /* sum of eweight over inMST (as verify(), :377)     */
   float ms_total;          /* device time of the whole solve (CUDA events)      */
   float ms_rounds;         /* device time of the round kernels                  */
   float ms_scan;           /* device time of the scan kernels                   */
-  /* device-clock breakdown (microseconds) taken at the kernels' barriers:   */
-  float us_scan[2][3];     /* per scan: flatten, vertex pass, chunk pass        */
+  /* breakdown (microseconds); us_scan from CUDA events, us_round from the
+   * device clock at the round kernel's barriers:                            */
+  float us_scan[2][3];     /* [0][0]: prep + light scan; [1][0]: flatten + heavy
+                              scan; the other slots are 0                      */
   float us_round[2][ECL_MAX_ROUNDS][2]; /* per round: find/min pass, mark pass  */
 } ecl_mst_stats;
 

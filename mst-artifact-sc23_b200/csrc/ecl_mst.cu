@@ -21,6 +21,7 @@ using namespace ecl;
 namespace {
 constexpr int kDefaultSplit = 8;
 constexpr unsigned kDefaultSmallTail = 4096;
+constexpr int64_t kWlSlack = 1 << 19;  // worklist slots beyond `edges` (scan chunk tails)
 constexpr int kLearnedMinEdges = 1 << 20;
 }  // namespace
 
@@ -129,8 +130,9 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   c->parent = (int*)(c->minv1 + max_nodes);
   // A phase's worklist holds at most one entry per one-direction CSR entry,
   // i.e. at most `edges` (the reference sizes it edges/2, :279, which only
-  // holds for symmetric inputs).
-  c->wl_cap = (unsigned)std::max<int64_t>(max_edges, 1);
+  // holds for symmetric inputs), plus slack for the unused tails of the
+  // scan warps' slot chunks.
+  c->wl_cap = (unsigned)std::max<int64_t>(max_edges + std::min<int64_t>(max_edges, kWlSlack), 1);
   for (int i = 0; i < 2; i++)
     if ((st = cuda_status(cudaMalloc(&c->wl[i], (size_t)c->wl_cap * sizeof(int4))))) return fail(st);
   c->first_v_cap = (int)(max_edges / kGran + 2);
@@ -205,16 +207,22 @@ int prepare_scan_kernels() {
 }
 
 // Persistent scan: exactly as many CTAs as can be resident at once (a CTA
-// started late would finish its share late), each looping over tiles.
+// started late would finish its share late), each looping over tiles. The
+// warps' slot chunk is sized so that the unused chunk tails (at most
+// chunk - 1 per warp) fit in the worklist's slack.
 template <int KIND, int EPT>
 int launch_scan_ept(const ScanArgs& sa, cudaStream_t s) {
-  const int m = sa.edges;
-  const int tiles = (int)((m + (int64_t)kScanThreads * EPT - 1) / ((int64_t)kScanThreads * EPT));
+  const int64_t m = sa.edges;
+  const int64_t tile = ScanCfg<EPT>::kTile;
+  const int tiles = (int)((m + tile - 1) / tile);
   int per_sm = 0;
   ECL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan<KIND, EPT>, kScanThreads,
                                                              scan_smem_bytes<EPT>()));
-  const int blocks = std::max(1, std::min(tiles, std::max(1, per_sm) * sa.sm_count));
-  k_scan<KIND, EPT><<<blocks, kScanThreads, scan_smem_bytes<EPT>(), s>>>(sa);
+  int blocks = std::max(1, std::min(tiles, std::max(1, per_sm) * sa.sm_count));
+  ScanArgs a = sa;
+  const int64_t warps = (int64_t)blocks * kScanWarps;
+  a.chunk = (unsigned)std::max<int64_t>(1, std::min<int64_t>(kScanMaxChunk, (int64_t)sa.wl_slack / warps));
+  k_scan<KIND, EPT><<<blocks, kScanThreads, scan_smem_bytes<EPT>(), s>>>(a);
   return cuda_status(cudaGetLastError());
 }
 
@@ -273,6 +281,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   sa.parent = c->parent;
   sa.wl = c->wl[0];
   sa.wl_cap = c->wl_cap;
+  sa.wl_slack = c->wl_cap - (unsigned)m;  // a scan keeps at most m entries
   sa.inMST = d_inMST;
   sa.vec_ok = ((((uintptr_t)g->nlist) | ((uintptr_t)g->eweight)) & 15) == 0;
   sa.zero_vec = (((uintptr_t)d_inMST) & 15) == 0;
@@ -321,16 +330,11 @@ int fill_stats(ecl_mst_ctx* c, ecl_mst_stats* stats, bool timed) {
   stats->rounds[1] = h.rounds[1];
   stats->status = (int32_t)h.error;
   for (int p = 0; p < 2; p++) {
-    stats->scan_kept[p] = h.wl_count[p][0];
+    stats->scan_kept[p] = h.scan_kept[p];
     for (int r = 0; r < ECL_MAX_ROUNDS; r++) stats->wl_in[p][r] = h.wl_count[p][r];
   }
   stats->atomics = (int64_t)h.atomics;
   for (int p = 0; p < 2; p++) {
-    if (h.t_scan[p][0] && h.t_scan[p][3]) {
-      stats->us_scan[p][0] = (h.t_scan[p][1] - h.t_scan[p][0]) * 1e-3f;
-      stats->us_scan[p][1] = (h.t_scan[p][2] - h.t_scan[p][1]) * 1e-3f;
-      stats->us_scan[p][2] = (h.t_scan[p][3] - h.t_scan[p][2]) * 1e-3f;
-    }
     u64 prev = h.t_round_start[p];
     for (int r = 0; r < h.rounds[p] && r < ECL_MAX_ROUNDS; r++) {
       const u64 a = h.t_round[p][2 * r], b = h.t_round[p][2 * r + 1];
@@ -349,6 +353,8 @@ int fill_stats(ecl_mst_ctx* c, ecl_mst_stats* stats, bool timed) {
     stats->ms_scan = t01 + t23;
     stats->ms_rounds = t12 + t34;
     stats->ms_total = t04;
+    stats->us_scan[0][0] = t01 * 1e3f;
+    stats->us_scan[1][0] = t23 * 1e3f;
   }
   return device_error_status(h.error);
 }
@@ -614,6 +620,8 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   sa.parent = parent;
   sa.wl = wl0;
   sa.wl_cap = (unsigned)kNaWlCap;
+  // within the stated limit a scan keeps at most m / 2 entries
+  sa.wl_slack = (unsigned)std::max<int64_t>(0, kNaWlCap - m / 2);
   sa.inMST = d_inMST;
   sa.vec_ok = ((((uintptr_t)g->nlist) | ((uintptr_t)g->eweight)) & 15) == 0;
   sa.zero_vec = (((uintptr_t)d_inMST) & 15) == 0;

@@ -10,12 +10,13 @@
 //
 //   k_prep        initPM + CSR checks + threshold choice + the tile->vertex
 //                 table of the edge-balanced scans
-//   k_scan<L,E>   initWL<true>: every thread takes E consecutive CSR entries
-//                 (128-bit loads); rows shorter than E stay inside one
-//                 thread, longer rows are spread over threads, warps and CTAs
-//                 (the reference's thread/warp degree split, :167/:185,
-//                 becomes the entries-per-thread E). Also zeroes inMST.
-//                 Appends are CTA-aggregated: one atomic per tile.
+//   k_scan<L,E>   initWL<true>: a producer warp stages CSR tiles into shared
+//                 memory with bulk asynchronous copies; every consumer lane
+//                 takes E consecutive entries, so rows shorter than E stay
+//                 inside one lane and longer rows are spread over lanes,
+//                 warps and CTAs (the reference's thread/warp degree split,
+//                 :167/:185, becomes the entries-per-lane E). Also zeroes
+//                 inMST. Appends are warp-aggregated, reserved in chunks.
 //   k_rounds      all Boruvka rounds of the phase in one cooperative launch
 //                 (kernel1, kernel2, kernel3 per round, bounded grid
 //                 barriers, no host round trip per round).
@@ -35,9 +36,7 @@
 namespace ecl {
 
 constexpr int kThreads = 512;          // threads of the prep, flatten and round kernels
-constexpr int kScanThreads = 256;      // threads of a scan CTA
-constexpr int kGran = kScanThreads * 4;// entries per tile->vertex table step
-constexpr int kSegCap = 4096;          // vertices of a tile's nindex slice kept in smem
+constexpr int kGran = 128;             // entries per tile->vertex table step (the smallest scan warp range)
 #ifndef ECL_ROUND_EPT
 #define ECL_ROUND_EPT 1
 #endif
@@ -88,6 +87,8 @@ struct ScanArgs {
   int vec_ok;    // nlist / eweight 16-byte aligned
   int zero_vec;  // inMST 16-byte aligned
   int sm_count;  // host side: sizes the persistent scan launch
+  unsigned wl_slack;  // host side: wl_cap minus the most entries a scan can keep
+  unsigned chunk;     // worklist slots a warp reserves at once (set at launch)
   DevState* st;
 };
 
@@ -230,237 +231,377 @@ __global__ void __launch_bounds__(kThreads) k_prep(PrepArgs a) {
 // ------------------------------------------------------------------ scans
 enum ScanKind { kLight = 0, kHeavy = 1 };
 
-// Edge-balanced CSR scan (initWL, ECL_MST.cu:157-207). Tile = kThreads * EPT
-// consecutive entries; thread t owns entries [tile0 + t*EPT, +EPT). The
-// vertex of each entry comes from the tile's slice of nindex in shared memory
-// (found through first_v), so hub rows and short rows cost the same per
-// entry. One-direction entries (nlist[j] > v) with the phase's weight test
-// are appended as {rep(v), rep(n), w, j}; the heavy scan additionally drops
-// entries whose endpoints share a light-phase tree (parent[] is flat, so a
-// rep is one load).
-// Asynchronous global -> shared copies (cp.async) of one tile: the thread's
-// own EPT entries of nlist and eweight (16-byte copies when aligned), and a
-// cooperative copy of the tile's nindex slice when it fits in shared memory.
-template <int EPT>
-__device__ __forceinline__ void scan_issue_tile(const ScanArgs& a, long long e0, int v_lo, int span,
-                                                int* nl_s, int* ew_s, int* sidx) {
-  const int m = a.edges;
-  const long long j0 = e0 + (long long)threadIdx.x * EPT;
-  int* nl_d = nl_s + threadIdx.x * EPT;
-  int* ew_d = ew_s + threadIdx.x * EPT;
-  if (a.vec_ok && j0 + EPT <= m) {
-#pragma unroll
-    for (int q = 0; q < EPT; q += 4) {
-      __pipeline_memcpy_async(nl_d + q, a.nlist + j0 + q, 16);
-      __pipeline_memcpy_async(ew_d + q, a.eweight + j0 + q, 16);
-    }
-  } else {
-    for (int q = 0; q < EPT && j0 + q < m; q++) {
-      __pipeline_memcpy_async(nl_d + q, a.nlist + j0 + q, 4);
-      __pipeline_memcpy_async(ew_d + q, a.eweight + j0 + q, 4);
-    }
-  }
-  if (span <= kSegCap)
-    for (int i = threadIdx.x; i <= span; i += blockDim.x) __pipeline_memcpy_async(sidx + i, a.nindex + v_lo + i, 4);
-  __pipeline_commit();
-}
+// Edge-balanced CSR scan (initWL, ECL_MST.cu:157-207), warp-specialised and
+// persistent. A tile is kScanWarps * 32 * EPT consecutive CSR entries. One
+// producer warp stages each tile's slices of nlist, eweight and nindex into a
+// ring of shared-memory stages with bulk asynchronous copies (cp.async.bulk;
+// completion counted on the stage's `full` mbarrier) and refills a stage once
+// every consumer warp has released it (`empty` mbarrier). Each consumer warp
+// takes 32 * EPT consecutive entries of the staged tile, EPT per lane, so hub
+// rows and short rows cost the same per entry (the reference's thread / warp
+// degree split, :167/:185, becomes the entries-per-lane EPT). A consumer
+// finds the vertex of its entries from the staged nindex slice alone: a
+// 32-ary search for the row holding the warp's first entry, the rows starting
+// inside the warp's range marked in a warp-private array, and a warp max-scan
+// over the marks; no step waits on the whole CTA. One-direction entries
+// (nlist[j] > v) passing the phase's weight test are appended as
+// {rep(v), rep(n), w, j}; the heavy scan also drops entries whose endpoints
+// share a light-phase tree (parent[] is flat, so a rep is one load).
+// Worklist slots are reserved per warp, `chunk` at a time, from the phase's
+// counter; the unused tail of each warp's last chunk is filled with null
+// entries (x = -1), which the first round skips.
+constexpr int kScanWarps = 8;                        // consumer warps of a scan CTA
+constexpr int kScanThreads = (kScanWarps + 1) * 32;  // plus the producer warp
+constexpr int kScanSegCap = 2048;                    // longest nindex slice (vertices) staged per tile
+constexpr unsigned kScanMaxChunk = 64;               // worklist slots a warp reserves at once
 
-// Persistent, double-buffered: while a CTA decides its current tile from
-// shared memory, the next tile's entries and nindex slice are already on
-// their way (cp.async), and the first_v pair of the tile after that is in
-// registers, so the only serial latency per tile is the reservation.
-// Dynamic shared memory of a scan CTA: two stages of (nlist, eweight) tiles
-// and two nindex slices.
+// ring stages and the resident CTAs per SM the launch bounds ask for, per EPT
+#ifndef ECL_SCAN_S4
+#define ECL_SCAN_S4 2
+#endif
+#ifndef ECL_SCAN_S8
+#define ECL_SCAN_S8 2
+#endif
+#ifndef ECL_SCAN_S16
+#define ECL_SCAN_S16 2
+#endif
+#ifndef ECL_SCAN_B4
+#define ECL_SCAN_B4 4
+#endif
+#ifndef ECL_SCAN_B8
+#define ECL_SCAN_B8 3
+#endif
+#ifndef ECL_SCAN_B16
+#define ECL_SCAN_B16 2
+#endif
+constexpr int kScanStages[3] = {ECL_SCAN_S4, ECL_SCAN_S8, ECL_SCAN_S16};
+constexpr int kScanMinB[3] = {ECL_SCAN_B4, ECL_SCAN_B8, ECL_SCAN_B16};
+
+template <int EPT>
+struct ScanCfg {
+  static constexpr int kIdx = EPT == 4 ? 0 : (EPT == 8 ? 1 : 2);
+  static constexpr int kTile = kScanWarps * 32 * EPT;  // entries per tile
+  static constexpr int kStages = kScanStages[kIdx];
+  static constexpr int kMinBlocks = kScanMinB[kIdx];
+  static constexpr int kSegInts = kScanSegCap + 8;         // slice from a 16-byte boundary
+  static constexpr int kStageInts = 2 * kTile + kSegInts;  // nlist, eweight, nindex slice
+  static constexpr size_t kHead = 128 + 48 * kStages;      // mbarriers, then stage headers
+  // stages, then one row-mark array of 32 * EPT ints per consumer warp
+  static constexpr size_t kSmem = kHead + sizeof(int) * ((size_t)kStages * kStageInts + kTile);
+};
+
 template <int EPT>
 constexpr size_t scan_smem_bytes() {
-  return 2 * 2 * (size_t)kScanThreads * EPT * sizeof(int) + 2 * (size_t)(kSegCap + 4) * sizeof(int) +
-         (size_t)kScanThreads * EPT * sizeof(int);
+  return ScanCfg<EPT>::kSmem;
+}
+
+struct ScanStage {
+  int v_lo;  // vertex holding the tile's first entry
+  int span;  // vertices v_lo .. v_lo + span - 1 may own the tile's entries
+  int off;   // nindex[v_lo] is at slice index off
+  int seg;   // 1 = nindex[v_lo .. v_lo + span] is staged
+  int wfirst[kScanWarps];  // vertex holding each consumer warp's first entry
+};
+static_assert(sizeof(ScanStage) == 48, "stage header size");
+
+// Largest v in [lo, lo + span) with nindex[v] <= e, for an entry e of a tile
+// whose rows are v_lo .. v_lo + span - 1 (global binary search; used when the
+// tile's slice is too long to stage).
+__device__ __forceinline__ int vertex_in(const int* nindex, int lo, int span, long long e) {
+  int hi = lo + span;
+  while (hi - lo > 1) {
+    const int mid = lo + ((hi - lo) >> 1);
+    if ((long long)__ldg(nindex + mid) <= e) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// The tiles a scan CTA takes, in order: first, first + step, ... < end.
+struct TileSeq {
+  int first, step, end;
+};
+__device__ __forceinline__ TileSeq scan_tiles(int ntiles) {
+#ifdef ECL_SCAN_CONTIG
+  const int g = gridDim.x, b = blockIdx.x, per = ntiles / g, rem = ntiles % g;
+  const int first = b * per + min(b, rem);
+  return TileSeq{first, 1, first + per + (b < rem ? 1 : 0)};
+#else
+  return TileSeq{(int)blockIdx.x, (int)gridDim.x, ntiles};
+#endif
+}
+
+// Producer warp: fills stage i % kStages with the CTA's i-th tile. The
+// 16-byte aligned bulk of each slice goes by bulk copy; a ragged end (the
+// last tile, the end of nindex) or unaligned arrays go by plain copies of the
+// warp's lanes, published by the same mbarrier arrival.
+template <int EPT>
+__device__ void scan_produce(const ScanArgs& a, unsigned char* smem, int ntiles) {
+  using C = ScanCfg<EPT>;
+  u64* full = reinterpret_cast<u64*>(smem);
+  u64* empty = full + C::kStages;
+  ScanStage* hdr = reinterpret_cast<ScanStage*>(smem + 128);
+  int* stages = reinterpret_cast<int*>(smem + C::kHead);
+  const int lane = threadIdx.x & 31;
+  const int n = a.nodes, m = a.edges;
+  const bool edge_bulk = a.vec_ok != 0;
+  const bool idx_bulk = (((uintptr_t)a.nindex) & 15) == 0;
+  // Lanes 0..7 read the vertex of each consumer warp's first entry, lane 8
+  // the vertex of the next tile's first entry (first_v has one entry per
+  // kGran entries), one tile ahead of the copies.
+  const TileSeq ts = scan_tiles(ntiles);
+  auto first_of = [&](int t) -> int {
+    if (lane > kScanWarps || t >= ts.end) return 0;
+    const int tb = t * (C::kTile / kGran) + lane * (32 * EPT / kGran);
+    return __ldg(a.first_v + min(tb, a.tiles));
+  };
+  int i = 0;
+  int cur = first_of(ts.first);
+  for (int t = ts.first; t < ts.end; t += ts.step, i++) {
+    const int s = i % C::kStages;
+    const int nxt = first_of(t + ts.step);
+    // every lane waits; the warp goes on only if all lanes saw the phase end
+    if (i >= C::kStages &&
+        !__all_sync(0xffffffffu, mbar_wait(&empty[s], ((i / C::kStages) - 1) & 1, kBarrierTimeoutNs))) {
+      if (lane == 0) atomicOr(&a.st->error, kErrTimeout);
+      break;
+    }
+    const int v_lo = __shfl_sync(0xffffffffu, cur, 0);
+    const int v_hi = __shfl_sync(0xffffffffu, cur, kScanWarps);
+    if (lane < kScanWarps) hdr[s].wfirst[lane] = cur;
+    cur = nxt;
+    const int span = v_hi - v_lo + 1;
+    const bool seg = span <= kScanSegCap;
+    const long long j0 = (long long)t * C::kTile;
+    const int cnt = (int)min((long long)C::kTile, (long long)m - j0);
+    int* nl = stages + (size_t)s * C::kStageInts;
+    int* ew = nl + C::kTile;
+    int* sx = ew + C::kTile;
+    const int a0 = v_lo & ~3, off = v_lo - a0;
+    const int want = seg ? off + span + 1 : 0;  // slice ints from a0 (a0 + want <= n + 1)
+    const int bulk_e = edge_bulk ? (cnt & ~3) : 0;
+    const int bulk_x = idx_bulk ? min((want + 3) & ~3, (n + 1 - a0) & ~3) : 0;
+    for (int q = bulk_e + lane; q < cnt; q += 32) {
+      nl[q] = __ldg(a.nlist + j0 + q);
+      ew[q] = __ldg(a.eweight + j0 + q);
+    }
+    for (int q = bulk_x + lane; q < want; q += 32) sx[q] = __ldg(a.nindex + a0 + q);
+    if (lane == 0) {
+      hdr[s].v_lo = v_lo;
+      hdr[s].span = span;
+      hdr[s].off = off;
+      hdr[s].seg = seg ? 1 : 0;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      fence_proxy_async_smem();
+      mbar_arrive_tx(&full[s], 4u * (unsigned)(2 * bulk_e + bulk_x));
+      if (bulk_e) {
+        bulk_g2s(nl, a.nlist + j0, 4u * (unsigned)bulk_e, &full[s]);
+        bulk_g2s(ew, a.eweight + j0, 4u * (unsigned)bulk_e, &full[s]);
+      }
+      if (bulk_x) bulk_g2s(sx, a.nindex + a0, 4u * (unsigned)bulk_x, &full[s]);
+    }
+  }
+  // Copies still in flight land before the CTA may exit.
+  if (lane == 0)
+    for (int k = max(0, i - C::kStages); k < i; k++)
+      if (!mbar_wait(&full[k % C::kStages], (k / C::kStages) & 1, kBarrierTimeoutNs))
+        atomicOr(&a.st->error, kErrTimeout);
 }
 
 template <int KIND, int EPT>
-__global__ void __launch_bounds__(kScanThreads, EPT == 16 ? 2 : 3) k_scan(ScanArgs a) {
-  constexpr int kTile = kScanThreads * EPT;
-  constexpr int kStep = EPT / 4;  // first_v entries per tile
-  extern __shared__ __align__(16) int scan_dyn[];
-  int (*nl_s)[kTile] = reinterpret_cast<int (*)[kTile]>(scan_dyn);
-  int (*ew_s)[kTile] = reinterpret_cast<int (*)[kTile]>(scan_dyn + 2 * kTile);
-  int (*sidx_s)[kSegCap + 4] = reinterpret_cast<int (*)[kSegCap + 4]>(scan_dyn + 4 * kTile);
-  // row-start marks of the current tile: (generation << 13) | (span index + 1)
-  int* rmark = scan_dyn + 4 * kTile + 2 * (kSegCap + 4);
-  __shared__ unsigned warp_off[kScanThreads / 32];
-  __shared__ unsigned tile_base;
+__global__ void __launch_bounds__(kScanThreads, ScanCfg<EPT>::kMinBlocks) k_scan(ScanArgs a) {
+  using C = ScanCfg<EPT>;
+  constexpr int kTile = C::kTile, R = 32 * EPT;  // entries per tile / per consumer warp
+  extern __shared__ __align__(128) unsigned char scan_dyn[];
+  u64* full = reinterpret_cast<u64*>(scan_dyn);
+  u64* empty = full + C::kStages;
+  const ScanStage* hdr = reinterpret_cast<const ScanStage*>(scan_dyn + 128);
+  const int* stages = reinterpret_cast<const int*>(scan_dyn + C::kHead);
   DevState* st = a.st;
   if (ld_volatile(&st->error) & kErrFormat) return;  // set by k_prep only
   if (KIND == kHeavy && !st->filtered) return;
   if (scan_ept(st->split) != EPT) return;  // only the variant the split selects runs
-  const int thr = st->threshold;
   const int n = a.nodes, m = a.edges;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int ntiles = (int)(((long long)m + kTile - 1) / kTile);
-  int t = blockIdx.x;
-  if (t >= ntiles) return;
-  const int stride = gridDim.x;
-  auto first_v = [&](int tile) -> int2 {
-    const int tb = tile * kStep;
-    return make_int2(__ldg(a.first_v + tb), __ldg(a.first_v + min(tb + kStep, a.tiles)));
-  };
-  int2 fv_cur = first_v(t);
-  int2 fv_nxt = t + stride < ntiles ? first_v(t + stride) : make_int2(0, 0);
-  scan_issue_tile<EPT>(a, (long long)t * kTile, fv_cur.x, fv_cur.y - fv_cur.x + 1, nl_s[0], ew_s[0], sidx_s[0]);
-  for (int q = threadIdx.x; q < kTile; q += blockDim.x) rmark[q] = 0;  // generation 0 never matches
-  int gen = 0;
-  __pipeline_wait_prior(0);
+  if ((int)blockIdx.x >= ntiles) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::kStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kScanWarps);
+    }
+    mbar_fence_init();
+  }
   __syncthreads();
-  for (int buf = 0; t < ntiles; t += stride, buf ^= 1) {
-    const int tn = t + stride;
-    if (tn < ntiles)
-      scan_issue_tile<EPT>(a, (long long)tn * kTile, fv_nxt.x, fv_nxt.y - fv_nxt.x + 1, nl_s[buf ^ 1],
-                           ew_s[buf ^ 1], sidx_s[buf ^ 1]);
-    const int2 fv_after = tn + stride < ntiles ? first_v(tn + stride) : make_int2(0, 0);
-    const long long e0 = (long long)t * kTile;
-    const long long j0 = e0 + (long long)threadIdx.x * EPT;
-    const int v_lo = fv_cur.x;
-    const int span = fv_cur.y - fv_cur.x + 1;  // vertices whose rows may hold this tile's entries
-    const bool seg = span <= kSegCap;
-    const int* sidx = sidx_s[buf];
-    auto row_start = [&](int i) -> int {  // nindex[v_lo + i]
-      return seg ? sidx[i] : __ldg(a.nindex + v_lo + i);
-    };
-    // the thread's own entries, 128 bits at a time from the staged tile
+  if (warp == kScanWarps) {
+    scan_produce<EPT>(a, scan_dyn, ntiles);
+    return;
+  }
+  // Row-start marks of this warp's range: row index minus the warp's first
+  // row, 0 = no row starts there. Each lane clears its own slots after use.
+  int* rmark = reinterpret_cast<int*>(scan_dyn + C::kHead) + (size_t)C::kStages * C::kStageInts + warp * R;
+  for (int q = lane; q < R; q += 32) rmark[q] = 0;
+  __syncwarp();
+  const int thr = st->threshold;
+  unsigned* ctr = &st->wl_count[KIND][0];
+  unsigned wpos = 0, wend = 0, kept = 0;  // this warp's reserved, unused slots [wpos, wend)
+  unsigned idmax = 0;                     // largest neighbour id seen, as unsigned
+  int i = 0;
+  const TileSeq ts = scan_tiles(ntiles);
+  for (int t = ts.first; t < ts.end; t += ts.step, i++) {
+    const int s = i % C::kStages;
+    if (!__all_sync(0xffffffffu, mbar_wait(&full[s], (i / C::kStages) & 1, kBarrierTimeoutNs))) {
+      if (lane == 0) atomicOr(&st->error, kErrTimeout);
+      break;
+    }
+    const int* nl = stages + (size_t)s * C::kStageInts;
+    const int v_lo = hdr[s].v_lo, span = hdr[s].span;
+    const int* sx = nl + 2 * kTile + hdr[s].off;  // sx[i] = nindex[v_lo + i]
+    // entry positions fit in 32 bits (edges < 2^31)
+    const unsigned jw = (unsigned)t * kTile + warp * R;  // first entry of this warp
+    const unsigned jl = jw + lane * EPT;                 // first entry of this lane
+    const int lim = jl < (unsigned)m ? min(EPT, m - (int)jl) : 0;  // the lane's valid entries
+    const int* nlw = nl + warp * R + lane * EPT;
+    const int* eww = nlw + kTile;
+    // the lane's entries, 128 bits at a time from the staged tile
     int nb[EPT], w[EPT];
-    if (j0 + EPT <= m) {
+    if (lim == EPT) {
 #pragma unroll
       for (int q = 0; q < EPT; q += 4) {
-        const int4 x = *reinterpret_cast<const int4*>(&nl_s[buf][threadIdx.x * EPT + q]);
-        const int4 y = *reinterpret_cast<const int4*>(&ew_s[buf][threadIdx.x * EPT + q]);
+        const int4 x = *reinterpret_cast<const int4*>(nlw + q);
+        const int4 y = *reinterpret_cast<const int4*>(eww + q);
         nb[q] = x.x; nb[q + 1] = x.y; nb[q + 2] = x.z; nb[q + 3] = x.w;
         w[q] = y.x; w[q + 1] = y.y; w[q + 2] = y.z; w[q + 3] = y.w;
       }
     } else {
 #pragma unroll
       for (int q = 0; q < EPT; q++) {
-        const bool in = j0 + q < m;
-        nb[q] = in ? nl_s[buf][threadIdx.x * EPT + q] : -1;
-        w[q] = in ? ew_s[buf][threadIdx.x * EPT + q] : 0;
+        nb[q] = q < lim ? nlw[q] : -1;
+        w[q] = q < lim ? eww[q] : 0;
       }
     }
-    if (KIND == kLight && j0 < m) {  // inMST = 0 (the reference memsets it, :306)
-      if (a.zero_vec && j0 + EPT <= m) {
-        if (EPT == 4) *reinterpret_cast<unsigned*>(a.inMST + j0) = 0u;
-        else if (EPT == 8) *reinterpret_cast<uint2*>(a.inMST + j0) = make_uint2(0u, 0u);
-        else *reinterpret_cast<uint4*>(a.inMST + j0) = make_uint4(0u, 0u, 0u, 0u);
-      } else {
-        for (int q = 0; q < EPT && j0 + q < m; q++) a.inMST[j0 + q] = 0;
-      }
-    }
-    // Vertex of every entry without a per-entry walk: each row starting
-    // inside the tile marks its start position with its span index (the
-    // largest index wins, so a run of zero-degree rows resolves to the row
-    // that owns the entries); an entry's vertex is then the largest mark at
-    // or before it, seeded with the vertex of the thread's first entry.
-    // (Tiles whose vertex range exceeds the shared slice, i.e. long runs of
-    // zero-degree vertices, search each entry in global nindex instead.)
-    auto last_row_at_or_before = [&](long long j) -> int {
-      int lo = 0, hi = span;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (row_start(mid) <= j) lo = mid;
-        else hi = mid;
-      }
-      return lo;
-    };
-    gen++;
-    if (seg)
-      for (int r = 1 + threadIdx.x; r < span; r += blockDim.x) {
-        const long long p = (long long)sidx[r] - e0;
-        if (p > 0 && p < kTile) atomicMax(&rmark[p], (gen << 13) | (r + 1));
-      }
-    const int i0 = j0 < m ? last_row_at_or_before(j0) : 0;  // vertex of entry j0
-    __syncthreads();
+    // Vertex of every entry, as an offset from v_lo.
     int vi[EPT];
-    if (seg) {
-      int run = i0;
+    if (hdr[s].seg) {
+      const int lo = hdr[s].wfirst[warp] - v_lo;  // row holding entry jw
+      // Rows starting inside (jw, jw + R) mark their start; of several rows
+      // starting at one position (zero-degree rows) the last one owns it.
+      if (jw < (unsigned)m)
+        for (int kb = lo + 1;; kb += 32) {
+          const int k = kb + lane;
+          const unsigned sk = k <= span ? (unsigned)sx[k] : jw + R;
+          const bool in = sk < jw + R;
+          if (in) atomicMax(&rmark[sk - jw], k - lo);
+          if (__ballot_sync(0xffffffffu, in) != 0xffffffffu) break;
+        }
+      __syncwarp();
+      // an entry's row is the last mark at or before it (lane-local running
+      // maximum, then a warp exclusive max-scan across lanes)
+      int run = 0, loc[EPT];
 #pragma unroll
       for (int q = 0; q < EPT; q += 4) {
-        const int4 mk = *reinterpret_cast<const int4*>(&rmark[threadIdx.x * EPT + q]);
-        const int c[4] = {mk.x, mk.y, mk.z, mk.w};
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          if ((c[u] >> 13) == gen) run = max(run, (c[u] & 8191) - 1);
-          vi[q + u] = run;
-        }
+        int4* slot = reinterpret_cast<int4*>(&rmark[lane * EPT + q]);
+        const int4 mk = *slot;
+        *slot = make_int4(0, 0, 0, 0);
+        loc[q] = run = max(run, mk.x);
+        loc[q + 1] = run = max(run, mk.y);
+        loc[q + 2] = run = max(run, mk.z);
+        loc[q + 3] = run = max(run, mk.w);
       }
-    } else {
+      int incl = run;
 #pragma unroll
-      for (int q = 0; q < EPT; q++) vi[q] = j0 + q < m ? last_row_at_or_before(j0 + q) : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl = max(incl, x);
+      }
+      int prev = __shfl_up_sync(0xffffffffu, incl, 1);
+      if (lane == 0) prev = 0;
+#pragma unroll
+      for (int q = 0; q < EPT; q++) vi[q] = lo + max(prev, loc[q]);
+    } else {
+      // slice too long to stage (long runs of zero-degree vertices)
+#pragma unroll
+      for (int q = 0; q < EPT; q++) vi[q] = q < lim ? vertex_in(a.nindex, v_lo, span, jl + q) - v_lo : 0;
     }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);  // this warp reads nothing more of the stage
+    if (KIND == kLight && lim > 0) {  // inMST = 0 (the reference memsets it, :306)
+      if (a.zero_vec && lim == EPT) {
+        if (EPT == 4) *reinterpret_cast<unsigned*>(a.inMST + jl) = 0u;
+        else if (EPT == 8) *reinterpret_cast<uint2*>(a.inMST + jl) = make_uint2(0u, 0u);
+        else *reinterpret_cast<uint4*>(a.inMST + jl) = make_uint4(0u, 0u, 0u, 0u);
+      } else {
+        for (int q = 0; q < lim; q++) a.inMST[jl + q] = 0;
+      }
+    }
+    // filter: one direction with a valid id (v < nb < n, as one unsigned
+    // compare), then the phase's weight test
+    unsigned cand = 0;
     int vtx[EPT], nrep[EPT];
-    unsigned keep = 0, cnt = 0;
-    int cur_v = -1, cur_rep = -1;
 #pragma unroll
     for (int q = 0; q < EPT; q++) {
-      const long long j = j0 + q;
-      vtx[q] = 0;
-      nrep[q] = nb[q];
-      if (j >= m) continue;
       const int v = v_lo + vi[q];
-      if ((unsigned)nb[q] >= (unsigned)n) {
-        atomicOr(&st->error, kErrFormat);
-        continue;
-      }
-      if (nb[q] <= v) continue;
-      if (KIND == kLight ? !(w[q] <= thr) : !(w[q] > thr)) continue;
-      int rv = v;
-      if (KIND == kHeavy) {
-        if (v != cur_v) {
-          cur_v = v;
-          cur_rep = __ldg(a.parent + v);
-        }
-        rv = cur_rep;
-        nrep[q] = __ldg(a.parent + nb[q]);
-        if (nrep[q] == rv) continue;
-      }
-      vtx[q] = rv;
-      keep |= 1u << q;
-      cnt++;
+      if (q < lim) idmax = max(idmax, (unsigned)nb[q]);
+      const bool pass = q < lim && (unsigned)nb[q] - (unsigned)v - 1u < (unsigned)(n - v - 1) &&
+                        (KIND == kLight ? w[q] <= thr : w[q] > thr);
+      cand |= (unsigned)pass << q;
+      vtx[q] = v;
+      nrep[q] = nb[q];
     }
-    // Tile reservation. Its two barriers double as the pipeline's: before
-    // the first, every thread has finished reading this tile's stage and has
-    // waited for its own copies of the next tile, so after it the next stage
-    // is complete and this one may be refilled.
+    if (KIND == kHeavy) {  // light-tree reps of both endpoints, all loads in flight together
+#pragma unroll
+      for (int q = 0; q < EPT; q++)
+        if (cand & (1u << q)) {
+          vtx[q] = __ldg(a.parent + vtx[q]);
+          nrep[q] = __ldg(a.parent + nb[q]);
+        }
+#pragma unroll
+      for (int q = 0; q < EPT; q++)
+        if (vtx[q] == nrep[q]) cand &= ~(1u << q);
+    }
+    const unsigned cnt = __popc(cand);
+    // warp reservation: slots from this warp's chunk, then a fresh chunk
     unsigned incl = cnt;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const unsigned x = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= o) incl += x;
     }
-    if (lane == 31) warp_off[warp] = incl;
-    __pipeline_wait_prior(0);
-    __syncthreads();
-    if (warp == 0) {
-      constexpr int nw = kScanThreads / 32;
-      const unsigned w0 = lane < nw ? warp_off[lane] : 0u;
-      unsigned x0 = w0;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned x = __shfl_up_sync(0xffffffffu, x0, o);
-        if (lane >= o) x0 += x;
+    const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total) {
+      const unsigned avail = wend - wpos;
+      unsigned fresh = 0, take = 0;
+      if (total > avail) {
+        take = max(total - avail, a.chunk);
+        if (lane == 0) fresh = atomicAdd(ctr, take);
+        fresh = __shfl_sync(0xffffffffu, fresh, 0);
       }
-      if (lane < nw) warp_off[lane] = x0 - w0;
-      if (lane == 31) tile_base = x0 ? atomicAdd(&st->wl_count[KIND][0], x0) : 0u;
-    }
-    __syncthreads();
-    unsigned pos = tile_base + warp_off[warp] + (incl - cnt);
+      unsigned p = incl - cnt;
 #pragma unroll
-    for (int q = 0; q < EPT; q++) {
-      if (!(keep & (1u << q))) continue;
-      if (pos < a.wl_cap) a.wl[pos] = make_int4(vtx[q], nrep[q], w[q], (int)(j0 + q));
-      else atomicOr(&st->error, kErrOverflow);
-      pos++;
+      for (int q = 0; q < EPT; q++) {
+        if (!(cand & (1u << q))) continue;
+        const unsigned slot = p < avail ? wpos + p : fresh + (p - avail);
+        if (slot < a.wl_cap) a.wl[slot] = make_int4(vtx[q], nrep[q], w[q], (int)(jl + q));
+        else atomicOr(&st->error, kErrOverflow);
+        p++;
+      }
+      if (total > avail) {
+        wpos = fresh + (total - avail);
+        wend = fresh + take;
+      } else {
+        wpos += total;
+      }
+      kept += cnt;
     }
-    fv_cur = fv_nxt;
-    fv_nxt = fv_after;
   }
+  if (idmax >= (unsigned)n) atomicOr(&st->error, kErrFormat);  // a neighbour id outside [0, n)
+  for (unsigned p = wpos + lane; p < wend; p += 32)  // null entries in the unused slots
+    if (p < a.wl_cap) a.wl[p] = make_int4(-1, -1, 0, 0);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+  if (lane == 0 && kept) atomicAdd(&st->scan_kept[KIND], kept);
 }
 
 // parent[v] = root(v) for every vertex, once before the heavy scan.
@@ -735,6 +876,7 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
       const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
       in_range[k] = idx < W;
       e[k] = in_range[k] ? __ldcg(in + idx) : make_int4(0, 0, 0, 0);
+      if (e[k].x < 0) in_range[k] = false;  // null entry (unused scan slot)
     }
     int v[N];
     bool vv[N];

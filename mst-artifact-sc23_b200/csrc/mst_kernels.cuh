@@ -43,7 +43,7 @@ struct DevState {
   // [phase][2r] after round r's find/min pass, [phase][2r+1] after its mark pass
   u64 t_round_start[2];
   u64 t_round[2][2 * ECL_MAX_ROUNDS];
-  u64 t_scan[2][4];  // start, after flatten, after pass 1, after pass 2
+  unsigned scan_kept[2];  // entries each scan kept (wl_count[p][0] also counts padding)
 };
 
 __device__ __forceinline__ u64 globaltimer_ns() {
@@ -87,6 +87,70 @@ __device__ __forceinline__ bool grid_barrier(DevState* st, u64 timeout_ns) {
   }
   __syncthreads();
   return (ld_volatile(&st->error) & kErrTimeout) == 0;
+}
+
+// ---- mbarriers and bulk asynchronous copies (cp.async.bulk, no multicast)
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(u64* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// Makes barrier initialisation visible to the asynchronous copy unit.
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(u64* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Arrive and add `bytes` to the transaction count the phase waits for.
+__device__ __forceinline__ void mbar_arrive_tx(u64* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+// Test for the phase's completion; if it is not complete the thread is
+// suspended until it completes or about 20 us pass (no busy spinning).
+__device__ __forceinline__ bool mbar_try_wait(u64* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(20000u)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for the phase of the given parity to complete, for at most
+// `timeout_ns`; false on expiry.
+__device__ __forceinline__ bool mbar_wait(u64* bar, unsigned parity, u64 timeout_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const u64 t0 = globaltimer_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (globaltimer_ns() - t0 > timeout_ns) return false;
+  return true;
+}
+
+// Orders this thread's generic-proxy shared-memory accesses before later
+// asynchronous-proxy (bulk copy) accesses.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Global -> shared bulk copy of `bytes` (multiple of 16, both addresses
+// 16-byte aligned); completion is counted on `bar`.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, u64* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
 }
 
 // Shared memory of one CTA-wide two-counter reservation.

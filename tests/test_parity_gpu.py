@@ -179,7 +179,13 @@ def test_stats_are_consistent(ctx):
     g = E.gen_rmat(16, 16, 0.57, 0.19, 0.19, 2, 1 << 24)
     _, st = ctx.run_host(g, E.make_opts(flags=E.FLAG_STATS))
     assert st["filtered"] == 1 and st["rounds"][0] > 0 and st["rounds"][1] > 0
-    assert st["scan_kept"][0] == st["wl_in"][0][0]
+    # the light scan keeps exactly the one-direction entries with w <= threshold
+    # (its worklist may add null padding after them, at most 63 slots per scan warp)
+    row = np.repeat(np.arange(g.nodes), np.diff(g.nindex))
+    light = int(np.count_nonzero((g.nlist > row) & (g.eweight <= st["threshold"])))
+    assert st["scan_kept"][0] == light
+    assert light <= st["wl_in"][0][0] <= light + 148 * 4 * 8 * 63
+    assert 0 < st["scan_kept"][1] <= st["wl_in"][1][0]
     assert st["atomics"] > 0
     assert st["ms_total"] > 0
     assert st["forest_edges"] <= g.nodes - 1
@@ -197,3 +203,71 @@ def test_rmat22_full_size_vs_oracle(ctx):
         assert np.array_equal(got, want), kw
         assert st["forest_weight"] == w
     big.close()
+
+
+def _csr_from_edges(n, u, v, w):
+    """Symmetric CSR (rows sorted by neighbour) from undirected edge arrays."""
+    src = np.concatenate([u, v]).astype(np.int64)
+    dst = np.concatenate([v, u]).astype(np.int64)
+    wt = np.concatenate([w, w]).astype(np.int32)
+    order = np.lexsort((dst, src))
+    src, dst, wt = src[order], dst[order], wt[order]
+    nindex = np.zeros(n + 1, np.int32)
+    np.add.at(nindex, src + 1, 1)
+    return E.Graph(np.cumsum(nindex).astype(np.int32), dst.astype(np.int32), wt)
+
+
+def test_long_zero_degree_runs(ctx):
+    """Tiles whose rows span more vertices than the staged nindex slice holds
+    (runs of thousands of isolated vertices between dense clusters) take the
+    global-search path; clusters of short rows between them take the staged one."""
+    rng = np.random.default_rng(5)
+    n = 300_000
+    clusters = [np.arange(0, 3000), np.arange(40_000, 40_050), np.arange(150_000, 152_000),
+                np.arange(299_000, 300_000)]
+    us, vs = [], []
+    for c in clusters:
+        k = len(c) * 6
+        us.append(rng.choice(c, k))
+        vs.append(rng.choice(c, k))
+    # a few long-range edges joining the clusters, and a hub
+    us.append(np.array([5, 40_010, 150_500, 299_999] + [7] * 500))
+    vs.append(np.array([40_020, 150_700, 299_500, 6] + list(rng.choice(n, 500))))
+    u, v = np.concatenate(us), np.concatenate(vs)
+    keep = u != v
+    u, v = u[keep], v[keep]
+    lo, hi = np.minimum(u, v), np.maximum(u, v)
+    pairs = np.unique(lo.astype(np.int64) * n + hi)
+    u, v = (pairs // n).astype(np.int64), (pairs % n).astype(np.int64)
+    w = rng.integers(1, 1000, len(u)).astype(np.int32)  # many ties
+    g = _csr_from_edges(n, u, v, w)
+    for kw in (dict(degree_split=1), dict(degree_split=8), dict(degree_split=1 << 20),
+               dict(mode=E.THRESH_NONE), dict(mode=E.THRESH_QUANTILE, quantile=0.3)):
+        o = E.make_opts(**kw)
+        got, st = ctx.run_host(g, o)
+        t, f = st["threshold"], st["filtered"]
+        want, _, _ = O.oracle_mst(g.nindex, g.nlist, g.eweight, t, f)
+        assert np.array_equal(got, want), kw
+
+
+def test_unaligned_device_buffers(ctx):
+    """CSR arrays and inMST starting 4 bytes past a 16-byte boundary: the scans
+    stage them with plain copies instead of bulk copies."""
+    import torch
+    g = E.gen_rmat(14, 16, 0.57, 0.19, 0.19, 4, 1 << 20)
+    want, _, _ = O.oracle_mst(g.nindex, g.nlist, g.eweight, *E.heuristic_threshold(g))
+    dev = torch.device("cuda:0")
+
+    def shifted(a):
+        buf = torch.zeros(len(a) + 1, dtype=torch.int32, device=dev)
+        buf[1:] = torch.from_numpy(a).to(dev)
+        return buf, buf[1:].data_ptr()
+
+    (bi, ni), (bl, nl), (bw, ew) = shifted(g.nindex), shifted(g.nlist), shifted(g.eweight)
+    out = torch.zeros(g.edges + 1, dtype=torch.uint8, device=dev)
+    for split in (1, 8, 1 << 20):
+        out.fill_(7)
+        ctx.run_device(g.nodes, g.edges, ni, nl, ew, out[1:].data_ptr(), opts=E.make_opts(degree_split=split))
+        ctx.sync()
+        got = out.cpu().numpy()
+        assert got[0] == 7 and np.array_equal(got[1:], want), split
