@@ -51,6 +51,7 @@ constexpr int kFindSlots = 1 << kFindLog;
 constexpr int kPairLog = 10;           // parallel-edge table: 1024 slots
 constexpr int kPairSlots = 1 << kPairLog;
 constexpr u64 kNoPair = ~0ull;
+constexpr int kSplitAfter = 8;         // find steps before path splitting starts
 constexpr unsigned long long kBarrierTimeoutNs = 5ull * 1000 * 1000 * 1000;
 
 // Entries per thread of the edge-balanced scan for a degree split: rows
@@ -731,41 +732,52 @@ __device__ __forceinline__ void drop_parallel_reserve(const int4 (&e)[E], bool (
 
 // Roots of the 2*kEPT endpoints a thread holds, all walks advanced in lock
 // step so their loads are in flight together. A per-CTA cache of
-// (vertex << 32 | root) absorbs repeated endpoints (roots do not change
-// during the find/min pass). Path splitting re-points each visited node to
-// its grandparent (stays inside the tree; bounds long hook chains).
+// (vertex << 32 | root) is consulted at every step (roots do not change
+// during the find/min pass): after a walk it holds the start vertex, its
+// parent and the root, so the nodes near the top of a large tree, which
+// every walk through that tree would otherwise read from the same L2 lines,
+// are read once per CTA. Hooking by random priority keeps trees shallow, so
+// a walk only starts path splitting (re-pointing each visited node to its
+// grandparent, which stays inside the tree) once it is kSplitAfter steps
+// deep: the writes bound pathological chains, while splitting every walk
+// would have the many walkers that share a start vertex all store to the
+// same parent entries.
+__device__ __forceinline__ int find_cached(const RoundSmem& s, int x) {
+  const u64 c = ((const volatile u64*)s.find_cache)[find_slot(x)];
+  return (int)(c >> 32) == x ? (int)(unsigned)c : -1;  // -1: not cached (x >= 0)
+}
+
 template <int N>
 __device__ __forceinline__ void multi_find(int (&v)[N], const bool (&valid)[N], int* parent,
                                            RoundSmem& s) {
-  int par[N];
+  int par[N], orig[N], first[N];  // first: the start vertex's parent
   unsigned miss = 0;
 #pragma unroll
   for (int i = 0; i < N; i++) {
+    orig[i] = v[i];
     par[i] = v[i];
+    first[i] = v[i];
     if (!valid[i]) continue;
-    const u64 c = ((volatile u64*)s.find_cache)[find_slot(v[i])];
-#ifdef ECL_NO_FINDCACHE
-    if (false) {
-#else
-    if ((int)(c >> 32) == v[i] && c != kNoEdge) {
-#endif
-      v[i] = (int)(unsigned)c;
-      par[i] = v[i];
+    const int r = find_cached(s, v[i]);
+    if (r >= 0) {
+      v[i] = par[i] = r;
     } else {
       miss |= 1u << i;
-      par[i] = __ldcg(parent + v[i]);
+      par[i] = first[i] = __ldcg(parent + v[i]);
     }
   }
-  int orig[N];
-#pragma unroll
-  for (int i = 0; i < N; i++) orig[i] = v[i];
-  for (;;) {
+  for (int step = 0;; step++) {
     int gp[N];
     bool any = false;
 #pragma unroll
     for (int i = 0; i < N; i++) {
       gp[i] = par[i];
       if (par[i] != v[i]) {
+        const int r = find_cached(s, par[i]);
+        if (r >= 0) {  // the rest of the walk is known
+          v[i] = par[i] = gp[i] = r;
+          continue;
+        }
         any = true;
         gp[i] = __ldcg(parent + par[i]);
       }
@@ -774,9 +786,7 @@ __device__ __forceinline__ void multi_find(int (&v)[N], const bool (&valid)[N], 
 #pragma unroll
     for (int i = 0; i < N; i++) {
       if (par[i] != v[i]) {
-#ifndef ECL_NO_SPLIT
-        if (gp[i] != par[i]) __stcg(parent + v[i], gp[i]);
-#endif
+        if (step >= kSplitAfter && gp[i] != par[i]) __stcg(parent + v[i], gp[i]);
         v[i] = par[i];
         par[i] = gp[i];
       }
@@ -784,8 +794,13 @@ __device__ __forceinline__ void multi_find(int (&v)[N], const bool (&valid)[N], 
   }
 #pragma unroll
   for (int i = 0; i < N; i++)
-    if (miss & (1u << i))
-      ((volatile u64*)s.find_cache)[find_slot(orig[i])] = ((u64)(unsigned)orig[i] << 32) | (unsigned)v[i];
+    if (miss & (1u << i)) {
+      volatile u64* fc = (volatile u64*)s.find_cache;
+      const u64 root = (unsigned)v[i];
+      fc[find_slot(orig[i])] = ((u64)(unsigned)orig[i] << 32) | root;
+      if (first[i] != v[i]) fc[find_slot(first[i])] = ((u64)(unsigned)first[i] << 32) | root;
+      if (orig[i] != v[i]) fc[find_slot(v[i])] = (root << 32) | root;
+    }
 }
 
 // Clear a previous-round min slot once per CTA.
@@ -800,7 +815,9 @@ __device__ __forceinline__ void reset_prev(int r, u64* mprev, RoundSmem& s) {
 // guarded atomicMin of ECL_MST.cu:221-223. Lanes of a warp holding the same
 // rep first reduce to the group minimum (warp-cooperative for high-degree
 // representatives); a group leader then folds it into the CTA's hot table.
-// Singletons, and leaders whose table slot belongs to another rep, read the
+// A lone entry of a rep already in the table folds into it as well, so a
+// giant component's rep costs no global traffic. The rest (lone entries of
+// other reps, leaders whose table slot belongs to another rep) read the
 // global slots together (one round trip for all pairs) and issue
 // fire-and-forget atomicMin only where the guard shows an improvement.
 // Every lane of the warp must call this.
@@ -817,12 +834,14 @@ __device__ __forceinline__ void offer_mins(const int (&rep)[N], const u64 (&key)
     cold[i] = false;
     val[i] = key[i];
     if (!valid[i]) continue;
-#ifdef ECL_NO_HOT
-    if (true) {
-#else
     if ((g & (g - 1)) == 0) {
-#endif
-      cold[i] = true;
+      // a lone entry of a rep already in the hot table folds into it too
+      const unsigned slot = hot_slot(rep[i]);
+      if (((volatile int*)s.hot_rep)[slot] == rep[i]) {
+        if (((volatile u64*)s.hot_key)[slot] > key[i]) atomicMin(&s.hot_key[slot], key[i]);
+      } else {
+        cold[i] = true;
+      }
       continue;
     }
     const unsigned khi = (unsigned)(key[i] >> 32);
