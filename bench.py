@@ -364,7 +364,7 @@ def main():
 
     # the same solve under the reference heuristic's schedule, for comparison
     heur_ms = []
-    if args.mode != "heuristic":
+    if args.mode != "heuristic" and not args.profile:
         for i in range(args.warmup + max(3, args.steps // 2)):
             flush.zero_()
             st_h = ctx.run_device(g.nodes, g.edges, d_ni.data_ptr(), d_nl.data_ptr(), d_ew.data_ptr(),
