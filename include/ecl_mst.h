@@ -174,13 +174,16 @@ typedef struct ecl_mst_stats {
   int64_t atomics;         /* guarded atomicMin issued (ECL_FLAG_STATS only)    */
   int64_t forest_edges;    /* number of inMST entries set                       */
   uint64_t forest_weight;  /* sum of eweight over inMST (as verify(), :377)     */
-  float ms_total;          /* device time of the whole solve (CUDA events)      */
+  float ms_total;          /* device time of the whole solve (CUDA events),
+                              the learned schedule's feature pass included      */
   float ms_rounds;         /* device time of the round kernels                  */
-  float ms_scan;           /* device time of the scan kernels                   */
+  float ms_scan;           /* device time of everything else (scans, prep,
+                              features, flatten)                                */
   /* breakdown (microseconds); us_scan from CUDA events, us_round from the
    * device clock at the round kernel's barriers:                            */
-  float us_scan[2][3];     /* [0][0]: prep + light scan; [1][0]: flatten + heavy
-                              scan; the other slots are 0                      */
+  float us_scan[2][3];     /* [0]: {features + prep + light scan, features +
+                              prep, light scan kernel}; [1]: {flatten + heavy
+                              scan, flatten, heavy scan kernel}                */
   float us_round[2][ECL_MAX_ROUNDS][2]; /* per round: find/min pass, mark pass  */
 } ecl_mst_stats;
 

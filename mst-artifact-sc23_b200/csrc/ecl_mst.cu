@@ -48,7 +48,9 @@ struct ecl_mst_ctx {
   int* d_nlist = nullptr;
   int* d_eweight = nullptr;
   unsigned char* d_inMST = nullptr;
-  cudaEvent_t ev[5] = {};
+  // timed solves: start, light scan end, light rounds end, heavy scan end, end,
+  // prep end, flatten end
+  cudaEvent_t ev[7] = {};
   // learned schedule: MLP parameters (and the load they came from), the 16
   // features, degree accumulators, the sorted 4096-entry weight sample
   float* ml_params = nullptr;
@@ -250,7 +252,6 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   const int split = o->degree_split > 0 ? o->degree_split : kDefaultSplit;
   const bool device_split = o->threshold_mode == ECL_THRESH_LEARNED;
   const int tiles = (int)(((int64_t)m + kGran - 1) / kGran);
-  if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[0], s));
   PrepArgs pa;
   pa.nodes = n;
   pa.edges = m;
@@ -302,6 +303,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   ra.count_atomics = (o->flags & ECL_FLAG_STATS) ? 1 : 0;
   const int rgrid = std::max(1, std::min(c->round_grid, (m / 2 + kThreads * kEPT - 1) / (kThreads * kEPT) + 1));
   int st;
+  if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[5], s));
   if ((st = launch_scans<kLight>(device_split, split, sa, s))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   ra.phase = 0;
@@ -310,6 +312,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   const int fgrid = (int)std::min<int64_t>(((int64_t)n + kThreads - 1) / kThreads, (int64_t)c->sm_count * 16);
   k_flatten<<<std::max(fgrid, 1), kThreads, 0, s>>>(c->parent, n, c->st);
   ECL_CUDA_TRY(cudaGetLastError());
+  if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[6], s));
   if ((st = launch_scans<kHeavy>(device_split, split, sa, s))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[3], s));
   ra.phase = 1;
@@ -353,8 +356,15 @@ int fill_stats(ecl_mst_ctx* c, ecl_mst_stats* stats, bool timed) {
     stats->ms_scan = t01 + t23;
     stats->ms_rounds = t12 + t34;
     stats->ms_total = t04;
+    float t05, t26;
+    cudaEventElapsedTime(&t05, c->ev[0], c->ev[5]);
+    cudaEventElapsedTime(&t26, c->ev[2], c->ev[6]);
     stats->us_scan[0][0] = t01 * 1e3f;
+    stats->us_scan[0][1] = t05 * 1e3f;
+    stats->us_scan[0][2] = (t01 - t05) * 1e3f;
     stats->us_scan[1][0] = t23 * 1e3f;
+    stats->us_scan[1][1] = t26 * 1e3f;
+    stats->us_scan[1][2] = (t23 - t26) * 1e3f;
   }
   return device_error_status(h.error);
 }
@@ -410,6 +420,8 @@ extern "C" int ecl_mst_run_device(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d
     return ECL_OK;
   }
   ECL_CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevState), s));
+  // the timed window starts before the learned schedule's feature pass
+  if (stats) ECL_CUDA_TRY(cudaEventRecord(c->ev[0], s));
   // Graphs below kLearnedMinEdges CSR entries keep the reference heuristic:
   // there the feature pass costs about as much as any schedule can save.
   if (o.threshold_mode == ECL_THRESH_LEARNED && g->edges < kLearnedMinEdges)
