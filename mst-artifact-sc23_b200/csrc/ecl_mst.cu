@@ -148,7 +148,7 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
     return fail(st);
   for (auto& e : c->ev)
     if ((st = cuda_status(cudaEventCreate(&e)))) return fail(st);
-  c->round_grid = coop_grid((const void*)k_rounds, kThreads, c->sm_count);
+  c->round_grid = coop_grid((const void*)k_rounds, kRoundThreads,c->sm_count);
   if ((st = prepare_scan_kernels())) return fail(st);
   if (c->round_grid <= 0) return fail(ECL_ERR_CUDA);
   *out = c;
@@ -301,13 +301,13 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   ra.small_tail = o->small_tail < 0 ? 0u : (o->small_tail == 0 ? kDefaultSmallTail : (unsigned)o->small_tail);
   if (o->flags & ECL_FLAG_NO_SMALL_TAIL) ra.small_tail = 0;
   ra.count_atomics = (o->flags & ECL_FLAG_STATS) ? 1 : 0;
-  const int rgrid = std::max(1, std::min(c->round_grid, (m / 2 + kThreads * kEPT - 1) / (kThreads * kEPT) + 1));
+  const int rgrid = std::max(1, std::min(c->round_grid, (m / 2 + kRoundThreads - 1) / kRoundThreads + 1));
   int st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[5], s));
   if ((st = launch_scans<kLight>(device_split, split, sa, s))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   ra.phase = 0;
-  if ((st = launch_coop((const void*)k_rounds, rgrid, kThreads, &ra, s))) return st;
+  if ((st = launch_coop((const void*)k_rounds, rgrid, kRoundThreads, &ra, s))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[2], s));
   const int fgrid = (int)std::min<int64_t>(((int64_t)n + kThreads - 1) / kThreads, (int64_t)c->sm_count * 16);
   k_flatten<<<std::max(fgrid, 1), kThreads, 0, s>>>(c->parent, n, c->st);
@@ -316,7 +316,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   if ((st = launch_scans<kHeavy>(device_split, split, sa, s))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[3], s));
   ra.phase = 1;
-  if ((st = launch_coop((const void*)k_rounds, rgrid, kThreads, &ra, s))) return st;
+  if ((st = launch_coop((const void*)k_rounds, rgrid, kRoundThreads, &ra, s))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[4], s));
   return ECL_OK;
 }
@@ -558,7 +558,7 @@ int na_setup(int dev, NaDevice** out) {
     ECL_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     if (!coop) return ECL_ERR_UNSUPPORTED;
     ECL_CUDA_TRY(cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev));
-    d.round_grid = coop_grid((const void*)k_rounds, kThreads, d.sm_count);
+    d.round_grid = coop_grid((const void*)k_rounds, kRoundThreads,d.sm_count);
     int ps = prepare_scan_kernels();
     if (ps) return ps;
     if (d.round_grid <= 0) return ECL_ERR_CUDA;
@@ -652,16 +652,16 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   ra.small_tail = o.small_tail < 0 ? 0u : (o.small_tail == 0 ? kDefaultSmallTail : (unsigned)o.small_tail);
   if (o.flags & ECL_FLAG_NO_SMALL_TAIL) ra.small_tail = 0;
   ra.count_atomics = (o.flags & ECL_FLAG_STATS) ? 1 : 0;
-  const int rgrid = std::max(1, std::min(d->round_grid, (m / 2 + kThreads * kEPT - 1) / (kThreads * kEPT) + 1));
+  const int rgrid = std::max(1, std::min(d->round_grid, (m / 2 + kRoundThreads - 1) / kRoundThreads + 1));
   if ((st = launch_scan<kLight>(scan_ept(split), sa, s))) return st;
   ra.phase = 0;
-  if ((st = launch_coop((const void*)k_rounds, rgrid, kThreads, &ra, s))) return st;
+  if ((st = launch_coop((const void*)k_rounds, rgrid, kRoundThreads, &ra, s))) return st;
   const int fgrid = (int)std::min<int64_t>(((int64_t)n + kThreads - 1) / kThreads, (int64_t)d->sm_count * 16);
   k_flatten<<<std::max(fgrid, 1), kThreads, 0, s>>>(parent, n, dst);
   ECL_CUDA_TRY(cudaGetLastError());
   if ((st = launch_scan<kHeavy>(scan_ept(split), sa, s))) return st;
   ra.phase = 1;
-  if ((st = launch_coop((const void*)k_rounds, rgrid, kThreads, &ra, s))) return st;
+  if ((st = launch_coop((const void*)k_rounds, rgrid, kRoundThreads, &ra, s))) return st;
   // Report device-side errors (malformed CSR, worklist overflow) to the caller.
   unsigned err = 0;
   ECL_CUDA_TRY(cudaMemcpyAsync(&err, &dst->error, sizeof(err), cudaMemcpyDeviceToHost, s));

@@ -35,20 +35,27 @@
 
 namespace ecl {
 
-constexpr int kThreads = 512;          // threads of the prep, flatten and round kernels
+constexpr int kThreads = 512;          // threads of the prep, flatten and batch kernels
 constexpr int kGran = 128;             // entries per tile->vertex table step (the smallest scan warp range)
-#ifndef ECL_ROUND_EPT
-#define ECL_ROUND_EPT 1
+#ifndef ECL_ROUND_THREADS
+#define ECL_ROUND_THREADS 512
 #endif
 #ifndef ECL_ROUND_MIN_BLOCKS
 #define ECL_ROUND_MIN_BLOCKS 4
 #endif
-constexpr int kEPT = ECL_ROUND_EPT;    // worklist entries per thread in a round tile
+#ifndef ECL_FIND_LOG
+#define ECL_FIND_LOG 10
+#endif
+#ifndef ECL_PAIR_LOG
+#define ECL_PAIR_LOG 10
+#endif
+constexpr int kRoundThreads = ECL_ROUND_THREADS;  // threads of a round CTA (one worklist entry each per tile)
+constexpr int kEPT = 1;                // worklist entries per thread in a round tile
 constexpr int kHotLog = 9;             // hot representative table: 512 slots
 constexpr int kHotSlots = 1 << kHotLog;
-constexpr int kFindLog = 10;           // find cache: 1024 slots
+constexpr int kFindLog = ECL_FIND_LOG; // find cache
 constexpr int kFindSlots = 1 << kFindLog;
-constexpr int kPairLog = 10;           // parallel-edge table: 1024 slots
+constexpr int kPairLog = ECL_PAIR_LOG; // parallel-edge table
 constexpr int kPairSlots = 1 << kPairLog;
 constexpr u64 kNoPair = ~0ull;
 constexpr int kSplitAfter = 8;         // find steps before path splitting starts
@@ -994,7 +1001,7 @@ __device__ __forceinline__ void round_mark(const RoundArgs& a, const int4* wl, u
   }
 }
 
-__global__ void __launch_bounds__(kThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(RoundArgs a) {
+__global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(RoundArgs a) {
   __shared__ RoundSmem s;
   DevState* st = a.st;
   const int ph = a.phase;
