@@ -283,6 +283,7 @@ def main():
     ap.add_argument("--split", type=int, default=0)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain ECL-MST comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-ablation", action="store_true", help="skip the technique-ablation leg")
     ap.add_argument("--batch", type=int, default=256,
                     help="graphs of the mixed batch to solve in batched mode (0 = skip)")
     ap.add_argument("--profile", action="store_true",
@@ -374,6 +375,37 @@ def main():
                                   stream=stream.cuda_stream, stats=True)
             if i >= args.warmup:
                 heur_ms.append(st_h["ms_total"])
+
+    # Ablation (the reference's deoptimization pipeline, generate_deoptimize_tables.py:6-14,
+    # restated for this engine): the reference heuristic schedule with techniques switched off,
+    # cumulatively for the reference's NoAtomicGuards / NoWarp / NoFilter steps, and one at a
+    # time for this engine's own techniques. Every variant must give the same inMST.
+    ablation = None
+    if not args.profile and not args.no_ablation:
+        E_ = E
+        series = [("base", 0, E_.THRESH_HEURISTIC),
+                  ("NAG", E_.FLAG_NO_GUARDS, E_.THRESH_HEURISTIC),
+                  ("NAG_NW", E_.FLAG_NO_GUARDS | E_.FLAG_NO_WARP_COOP, E_.THRESH_HEURISTIC),
+                  ("NAG_NW_NF", E_.FLAG_NO_GUARDS | E_.FLAG_NO_WARP_COOP, E_.THRESH_NONE),
+                  ("with_dedup", E_.FLAG_DEDUP, E_.THRESH_HEURISTIC),
+                  ("no_find_cache", E_.FLAG_NO_FIND_CACHE, E_.THRESH_HEURISTIC),
+                  ("no_small_tail", E_.FLAG_NO_SMALL_TAIL, E_.THRESH_HEURISTIC)]
+        ablation, base_ms, ref_hash = {}, None, None
+        for name, flags, tmode in series:
+            o = E_.make_opts(mode=tmode, degree_split=args.split, flags=flags)
+            ms = []
+            for i in range(2 + 5):
+                flush.zero_()
+                st_a = ctx.run_device(g.nodes, g.edges, d_ni.data_ptr(), d_nl.data_ptr(), d_ew.data_ptr(),
+                                      d_out.data_ptr(), opts=o, stream=stream.cuda_stream, stats=True)
+                if i >= 2:
+                    ms.append(st_a["ms_total"])
+            h = hash(d_out[: g.edges].cpu().numpy().tobytes())
+            ref_hash = h if ref_hash is None else ref_hash
+            m = float(np.mean(ms))
+            base_ms = m if base_ms is None else base_ms
+            ablation[name] = {"ms": m, "gedges_s": g.edges / (m * 1e-3) / 1e9, "slowdown": m / base_ms,
+                              "inMST_identical": h == ref_hash}
 
     # one extra solve counting the guarded atomics for the byte model
     st_atom = ctx.run_device(g.nodes, g.edges, d_ni.data_ptr(), d_nl.data_ptr(), d_ew.data_ptr(),
@@ -494,6 +526,7 @@ def main():
             # per solve: k_prep, k_scan x2, k_rounds x2, k_flatten; the learned schedule adds
             # k_feat_degrees, k_feat_finish, k_mlp_apply and launches all three scan variants
             "gpu_launches": (13 if args.mode == "learned" else 6) * args.steps,
+            "ablation": ablation,
             "heuristic_schedule": ({"value": world * g.edges / (np.mean(heur_ms) * 1e-3) / 1e9,
                                     "ms": float(np.mean(heur_ms)),
                                     "what": "same solve with the reference threshold heuristic"}

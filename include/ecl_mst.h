@@ -132,7 +132,18 @@ int ecl_heuristic_threshold(const ecl_graph* g, int32_t* threshold,
 enum {
   ECL_FLAG_L2_PERSIST = 1 << 0, /* L2 access-policy window on parent/min slots   */
   ECL_FLAG_STATS = 1 << 1,      /* count guarded atomics (slower; off in timing) */
-  ECL_FLAG_NO_SMALL_TAIL = 1 << 2 /* keep every round grid-wide (ablation)      */
+  ECL_FLAG_NO_SMALL_TAIL = 1 << 2, /* keep every round grid-wide (ablation)     */
+  /* Ablation switches: each turns one technique of the round kernel off, to
+   * measure what it buys (the answer is unchanged). NO_GUARDS is the
+   * reference's NoAtomicGuards variant (Deoptimizations/
+   * ECL_MST_NoAtomicGuards.cu:222-223); NO_WARP_COOP stands for its NoWarp
+   * variant, applied to this engine's warp/CTA cooperation on shared reps. */
+  ECL_FLAG_NO_GUARDS = 1 << 3,     /* atomicMin without reading the slot first  */
+  ECL_FLAG_NO_WARP_COOP = 1 << 4,  /* no warp reduction / CTA table for shared reps */
+  ECL_FLAG_DEDUP = 1 << 5,         /* per-tile parallel-edge elimination in the
+                                      rounds (off by default: on RMAT it costs
+                                      more than the smaller worklists save)     */
+  ECL_FLAG_NO_FIND_CACHE = 1 << 6  /* no per-CTA root cache in the finds        */
 };
 
 typedef struct mst_opts {

@@ -27,6 +27,7 @@ struct BatchArgs {
   int mode, explicit_thr;
   float quantile;
   int count_atomics;
+  unsigned abl;                 // round-kernel ablation switches (kAbl*)
 };
 
 // Threshold of one graph by the chosen rule (the reference heuristic per
@@ -245,6 +246,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_small(BatchArgs b) {
     ra.st = b.st;
     ra.small_tail = 0;
     ra.count_atomics = b.count_atomics;
+    ra.abl = b.abl;
     cta_scan<kLight>(ni, nl, ew, n, m, thr, parent, wl0, ra.wl_cap, &cnt[0], out, b.st, s.rs);
     __syncthreads();
     cta_rounds(ra, cnt, s);

@@ -92,6 +92,12 @@ int coop_grid(const void* fn, int threads, int sm_count) {
 
 int prepare_scan_kernels();
 
+// Round-kernel ablation bits from the option flags.
+unsigned round_ablation(int flags) {
+  return ((flags & ECL_FLAG_NO_GUARDS) ? kAblNoGuards : 0u) | ((flags & ECL_FLAG_NO_WARP_COOP) ? kAblNoCoop : 0u) |
+         ((flags & ECL_FLAG_DEDUP) ? kDedup : 0u) | ((flags & ECL_FLAG_NO_FIND_CACHE) ? kAblNoFindCache : 0u);
+}
+
 }  // namespace
 
 extern "C" void ecl_default_opts(mst_opts* o) {
@@ -301,6 +307,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   ra.small_tail = o->small_tail < 0 ? 0u : (o->small_tail == 0 ? kDefaultSmallTail : (unsigned)o->small_tail);
   if (o->flags & ECL_FLAG_NO_SMALL_TAIL) ra.small_tail = 0;
   ra.count_atomics = (o->flags & ECL_FLAG_STATS) ? 1 : 0;
+  ra.abl = round_ablation(o->flags);
   const int rgrid = std::max(1, std::min(c->round_grid, (m / 2 + kRoundThreads - 1) / kRoundThreads + 1));
   int st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[5], s));
@@ -652,6 +659,7 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   ra.small_tail = o.small_tail < 0 ? 0u : (o.small_tail == 0 ? kDefaultSmallTail : (unsigned)o.small_tail);
   if (o.flags & ECL_FLAG_NO_SMALL_TAIL) ra.small_tail = 0;
   ra.count_atomics = (o.flags & ECL_FLAG_STATS) ? 1 : 0;
+  ra.abl = round_ablation(o.flags);
   const int rgrid = std::max(1, std::min(d->round_grid, (m / 2 + kRoundThreads - 1) / kRoundThreads + 1));
   if ((st = launch_scan<kLight>(scan_ept(split), sa, s))) return st;
   ra.phase = 0;
@@ -836,6 +844,7 @@ int batch_enqueue(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST, const 
     ba.explicit_thr = o->threshold;
     ba.quantile = o->quantile;
     ba.count_atomics = (o->flags & ECL_FLAG_STATS) ? 1 : 0;
+    ba.abl = round_ablation(o->flags);
     const int grid = std::min(c->small_grid, S);
     k_batch_small<<<grid, kThreads, 0, s>>>(ba);
     ECL_CUDA_TRY(cudaGetLastError());

@@ -113,6 +113,15 @@ struct RoundArgs {
   DevState* st;
   unsigned small_tail;
   int count_atomics;
+  unsigned abl;  // kAbl* bits: techniques switched off to measure what they buy
+};
+
+// Ablation switches of the round kernel (mst_opts flags ECL_FLAG_NO_*).
+enum : unsigned {
+  kAblNoGuards = 1u,     // atomicMin without first reading the slot (ECL_MST.cu:222-223)
+  kAblNoCoop = 2u,       // no warp reduction or CTA table for shared reps
+  kDedup = 4u,           // parallel-edge elimination on (opt-in: measured slower on RMAT)
+  kAblNoFindCache = 8u,  // no per-CTA root cache in the finds
 };
 
 // ------------------------------------------------------------------ prep
@@ -654,19 +663,22 @@ __device__ __forceinline__ unsigned pair_slot(u64 pk) {
   return (unsigned)((pk * 0x9E3779B97F4A7C15ull) >> (64 - kPairLog));
 }
 
-// Parallel-edge elimination in the contracted graph, fused with the tile's
-// worklist reservation. Entries of one tile that join the same two trees are
-// parallel edges of the contracted graph; only the one with the smallest
-// (weight, j) key can be a forest edge (any forest through a heavier one is
-// heavier than the same forest through the lightest), so the others are
-// dropped for good. Warp groups with equal rep pairs reduce first; group
-// minima meet in a per-tile shared table. keep[k] is narrowed to the
-// survivors, and *pos receives the first output slot of this thread's
-// survivors (one global atomic per CTA tile). Three CTA barriers in all.
+// The tile's worklist reservation, optionally fused with parallel-edge
+// elimination (`dedup`, opt-in through ECL_FLAG_DEDUP). Entries of one tile
+// that join the same two trees are parallel edges of the contracted graph;
+// only the one with the smallest (weight, j) key can be a forest edge (any
+// forest through a heavier one is heavier than the same forest through the
+// lightest), so the others may be dropped for good. Warp groups with equal
+// rep pairs reduce first; group minima meet in a per-tile shared table.
+// Measured on RMAT scale 22 the elimination costs more (a third CTA barrier
+// and the table per tile) than the smaller worklists save, so it is off by
+// default. keep[k] is narrowed to the survivors, and *pos receives the first
+// output slot of this thread's survivors (one global atomic per CTA tile).
 // Every thread of the CTA must call this.
 template <int E>
 __device__ __forceinline__ void drop_parallel_reserve(const int4 (&e)[E], bool (&keep)[E],
-                                                      unsigned* ctr, RoundSmem& s, unsigned* pos) {
+                                                      unsigned* ctr, RoundSmem& s, unsigned* pos,
+                                                      bool dedup) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   u64 pk[E], gmin[E];
 #pragma unroll
@@ -675,7 +687,7 @@ __device__ __forceinline__ void drop_parallel_reserve(const int4 (&e)[E], bool (
     pk[k] = keep[k] ? (((u64)lo << 32) | hi) : (0xFFFFFFFF00000000ull | (threadIdx.x * E + k));
     const u64 key = edge_key(e[k].z, e[k].w);
     gmin[k] = key;
-#ifndef ECL_NO_DEDUP
+    if (!dedup) continue;  // uniform across the CTA
     const unsigned g = __match_any_sync(0xffffffffu, pk[k]);
     if (!keep[k]) continue;
     if (g & (g - 1)) {
@@ -693,20 +705,17 @@ __device__ __forceinline__ void drop_parallel_reserve(const int4 (&e)[E], bool (
       }
       if (t == pk[k] && ((volatile u64*)s.pair_min)[slot] > gmin[k]) atomicMin(&s.pair_min[slot], gmin[k]);
     }
-#endif
   }
-  __syncthreads();  // S1: the tile's pair table is complete
+  if (dedup) __syncthreads();  // S1: the tile's pair table is complete
   unsigned cnt = 0;
 #pragma unroll
   for (int k = 0; k < E; k++) {
-#ifndef ECL_NO_DEDUP
-    if (keep[k]) {
+    if (dedup && keep[k]) {
       const unsigned slot = pair_slot(pk[k]);
       const u64 key = edge_key(e[k].z, e[k].w);
       const u64 best = s.pair_tag[slot] == pk[k] ? s.pair_min[slot] : gmin[k];
       keep[k] = key == best;
     }
-#endif
     cnt += keep[k];
   }
   unsigned incl = cnt;
@@ -717,10 +726,11 @@ __device__ __forceinline__ void drop_parallel_reserve(const int4 (&e)[E], bool (
   }
   if (lane == 31) s.rs.warp_off[warp][0] = incl;
   __syncthreads();  // S2: every check done, warp totals written
-  for (int i = threadIdx.x; i < kPairSlots; i += blockDim.x) {
-    s.pair_tag[i] = kNoPair;
-    s.pair_min[i] = kNoEdge;
-  }
+  if (dedup)
+    for (int i = threadIdx.x; i < kPairSlots; i += blockDim.x) {
+      s.pair_tag[i] = kNoPair;
+      s.pair_min[i] = kNoEdge;
+    }
   if (warp == 0) {
     const int nw = blockDim.x >> 5;
     const unsigned w0 = lane < nw ? s.rs.warp_off[lane][0] : 0u;
@@ -756,7 +766,7 @@ __device__ __forceinline__ int find_cached(const RoundSmem& s, int x) {
 
 template <int N>
 __device__ __forceinline__ void multi_find(int (&v)[N], const bool (&valid)[N], int* parent,
-                                           RoundSmem& s) {
+                                           RoundSmem& s, bool use_cache = true) {
   int par[N], orig[N], first[N];  // first: the start vertex's parent
   unsigned miss = 0;
 #pragma unroll
@@ -765,7 +775,7 @@ __device__ __forceinline__ void multi_find(int (&v)[N], const bool (&valid)[N], 
     par[i] = v[i];
     first[i] = v[i];
     if (!valid[i]) continue;
-    const int r = find_cached(s, v[i]);
+    const int r = use_cache ? find_cached(s, v[i]) : -1;
     if (r >= 0) {
       v[i] = par[i] = r;
     } else {
@@ -780,7 +790,7 @@ __device__ __forceinline__ void multi_find(int (&v)[N], const bool (&valid)[N], 
     for (int i = 0; i < N; i++) {
       gp[i] = par[i];
       if (par[i] != v[i]) {
-        const int r = find_cached(s, par[i]);
+        const int r = use_cache ? find_cached(s, par[i]) : -1;
         if (r >= 0) {  // the rest of the walk is known
           v[i] = par[i] = gp[i] = r;
           continue;
@@ -801,7 +811,7 @@ __device__ __forceinline__ void multi_find(int (&v)[N], const bool (&valid)[N], 
   }
 #pragma unroll
   for (int i = 0; i < N; i++)
-    if (miss & (1u << i)) {
+    if (use_cache && (miss & (1u << i))) {
       volatile u64* fc = (volatile u64*)s.find_cache;
       const u64 root = (unsigned)v[i];
       fc[find_slot(orig[i])] = ((u64)(unsigned)orig[i] << 32) | root;
@@ -831,15 +841,18 @@ __device__ __forceinline__ void reset_prev(int r, u64* mprev, RoundSmem& s) {
 template <int N>
 __device__ __forceinline__ void offer_mins(const int (&rep)[N], const u64 (&key)[N],
                                            const bool (&valid)[N], u64* mcur, RoundSmem& s,
-                                           unsigned long long& atomics) {
+                                           unsigned long long& atomics, bool coop = true,
+                                           bool guard = true) {
   const int lane = threadIdx.x & 31;
   bool cold[N];
   u64 val[N];
 #pragma unroll
   for (int i = 0; i < N; i++) {
-    const unsigned g = __match_any_sync(0xffffffffu, valid[i] ? rep[i] : -2 - lane);
-    cold[i] = false;
+    cold[i] = valid[i];
     val[i] = key[i];
+    if (!coop) continue;  // uniform: every valid pair goes straight to its global slot
+    cold[i] = false;
+    const unsigned g = __match_any_sync(0xffffffffu, valid[i] ? rep[i] : -2 - lane);
     if (!valid[i]) continue;
     if ((g & (g - 1)) == 0) {
       // a lone entry of a rep already in the hot table folds into it too
@@ -871,7 +884,7 @@ __device__ __forceinline__ void offer_mins(const int (&rep)[N], const u64 (&key)
   }
   u64 seen[N];
 #pragma unroll
-  for (int i = 0; i < N; i++) seen[i] = cold[i] ? __ldcg(mcur + rep[i]) : 0ull;
+  for (int i = 0; i < N; i++) seen[i] = cold[i] && guard ? __ldcg(mcur + rep[i]) : kNoEdge;
 #pragma unroll
   for (int i = 0; i < N; i++) {
     if (cold[i] && seen[i] > val[i]) {
@@ -916,7 +929,7 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
         reset_prev(e[k].y, mprev, s);
       }
     }
-    multi_find<N>(v, vv, a.parent, s);
+    multi_find<N>(v, vv, a.parent, s, !(a.abl & kAblNoFindCache));
     bool keep[kEPT];
 #pragma unroll
     for (int k = 0; k < kEPT; k++) {
@@ -925,7 +938,7 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
       e[k].y = v[2 * k + 1];
     }
     unsigned pos;
-    drop_parallel_reserve<kEPT>(e, keep, out_ctr, s, &pos);
+    drop_parallel_reserve<kEPT>(e, keep, out_ctr, s, &pos, (a.abl & kDedup) != 0);
     u64 key[N];
     bool kv[N];
 #pragma unroll
@@ -938,7 +951,7 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
       key[2 * k] = key[2 * k + 1] = edge_key(e[k].z, e[k].w);
       kv[2 * k] = kv[2 * k + 1] = keep[k];
     }
-    offer_mins<N>(v, key, kv, mcur, s, atomics);
+    offer_mins<N>(v, key, kv, mcur, s, atomics, !(a.abl & kAblNoCoop), !(a.abl & kAblNoGuards));
   }
   __syncthreads();
   // flush the CTA's partial minima of hot representatives
@@ -946,7 +959,7 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
     const int r = s.hot_rep[i];
     if (r >= 0) {
       const u64 k = s.hot_key[i];
-      if (__ldcg(mcur + r) > k) {
+      if ((a.abl & kAblNoGuards) || __ldcg(mcur + r) > k) {
         atomicMin(mcur + r, k);
         atomics++;
       }

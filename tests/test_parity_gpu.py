@@ -21,6 +21,13 @@ MODES = [
     dict(small_tail=-1),
     dict(small_tail=1 << 30),
     dict(mode=E.THRESH_QUANTILE, quantile=0.3, degree_split=2, small_tail=-1),
+    # ablation switches: each turns a technique off; the answer must not change
+    dict(flags=E.FLAG_NO_GUARDS),
+    dict(flags=E.FLAG_NO_WARP_COOP),
+    dict(flags=E.FLAG_DEDUP),
+    dict(flags=E.FLAG_NO_FIND_CACHE),
+    dict(flags=E.FLAG_NO_GUARDS | E.FLAG_NO_WARP_COOP | E.FLAG_DEDUP | E.FLAG_NO_FIND_CACHE
+         | E.FLAG_NO_SMALL_TAIL, mode=E.THRESH_NONE),
 ]
 
 
