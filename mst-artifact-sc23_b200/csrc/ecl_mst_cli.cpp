@@ -6,18 +6,50 @@
 // on the device and ends when the forest is complete; weights are synthesised
 // for weightless inputs (:410-419) and the threshold is the reference
 // heuristic (:432-444). A last line reports the forest size and weight.
+//
+// An optional third argument names a deoptimized variant the way the
+// reference's ablation binaries are named (Deoptimizations/
+// run_all_ECL-MST_deopts.sh): "NAG", "NAG_NW", "NAG_NW_NF" switch off the
+// atomic guards, the warp cooperation and the filter of this engine (the
+// forest is unchanged). The reference's later steps (NIPC, NOD, NT, NDD,
+// NEB) remove structure this engine is built on and are not reproduced.
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
+#include <string>
 #include <vector>
 
 #include "ecl_mst.h"
 
+// Options of a named variant; false if a component is not reproduced.
+static bool variant_opts(const char* name, mst_opts* o) {
+  ecl_default_opts(o);
+  std::string s(name);
+  size_t pos = 0;
+  while (pos <= s.size()) {
+    const size_t end = s.find('_', pos);
+    const std::string part = s.substr(pos, end == std::string::npos ? std::string::npos : end - pos);
+    if (part == "NAG") o->flags |= ECL_FLAG_NO_GUARDS;
+    else if (part == "NW") o->flags |= ECL_FLAG_NO_WARP_COOP;
+    else if (part == "NF") o->threshold_mode = ECL_THRESH_NONE;
+    else if (part != "base") return false;
+    if (end == std::string::npos) break;
+    pos = end + 1;
+  }
+  return true;
+}
+
 int main(int argc, char* argv[]) {
-  if (argc < 2 || argc > 3) {
-    printf("USAGE: %s input_graph [runs]\n", argv[0]);
+  if (argc < 2 || argc > 4) {
+    printf("USAGE: %s input_graph [runs] [variant: base | NAG | NAG_NW | NAG_NW_NF]\n", argv[0]);
     return 1;
   }
-  const int runs = argc == 3 ? atoi(argv[2]) : 9;
+  const int runs = argc >= 3 ? atoi(argv[2]) : 9;
+  mst_opts opts;
+  if (!variant_opts(argc == 4 ? argv[3] : "base", &opts)) {
+    fprintf(stderr, "ERROR: variant %s is not reproduced by this engine\n", argv[3]);
+    return 1;
+  }
   ecl_graph g;
   int st = ecl_read_graph(argv[1], &g);
   if (st) {
@@ -40,7 +72,7 @@ int main(int argc, char* argv[]) {
   std::vector<uint8_t> inMST((size_t)(g.edges > 0 ? g.edges : 1));
   ecl_mst_stats stats;
   for (int i = 0; i < runs; i++) {
-    if ((st = ecl_mst_ctx_run_host(ctx, &g, inMST.data(), nullptr, &stats))) {
+    if ((st = ecl_mst_ctx_run_host(ctx, &g, inMST.data(), &opts, &stats))) {
       fprintf(stderr, "ERROR: %s\n", ecl_status_string(st));
       return 1;
     }

@@ -278,3 +278,27 @@ def test_unaligned_device_buffers(ctx):
         ctx.sync()
         got = out.cpu().numpy()
         assert got[0] == 7 and np.array_equal(got[1:], want), split
+
+
+def test_cli_variants_and_table_pipeline(tmp_path):
+    """The drop-in CLI prints the reference binary's blocks (input line + one
+    runtime per run) for each deoptimized variant it reproduces; the table port
+    reads them; every variant reports the same forest."""
+    import os
+    import subprocess
+    import compare_tables as T
+    exe = os.path.join(os.path.dirname(E.LIB_PATH), "ecl_mst")
+    g = E.gen_rmat(14, 16, 0.57, 0.19, 0.19, 5, 1 << 20)
+    path = str(tmp_path / "rmat14.egr")
+    E.write_graph(g, path)
+    outs, forests = {}, set()
+    for v in ("base", "NAG", "NAG_NW", "NAG_NW_NF"):
+        r = subprocess.run([exe, path, "3", v], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr
+        outs[f"ecl_mst_{v}_out.csv"] = r.stdout
+        forests.add(r.stdout.strip().splitlines()[-1])
+    assert len(forests) == 1
+    inputs, names, rt, tp = T.tables(outs, runs=3)
+    assert len(inputs) == 1 and all(x is not None and x > 0 for x in tp[0])
+    r = subprocess.run([exe, path, "3", "NAG_NW_NF_NIPC"], capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0
