@@ -177,14 +177,22 @@ def scan_kernel_bytes(st, nodes, edges, entry_bytes=16):
     return b
 
 
-def batch_leg(args, E, torch, dev):
+def batch_leg(args, E, torch, dev, rank=0, world=1, dist=None):
     """Mixed-family batch (graphs seeded 1000, 1001, ...; sizes log-uniform in
     [1e3, 2e6] vertices; grid / ER deg 8 / RMAT ef 8 / RGG2D deg 3; weights
     U[1, 2^20]): the first `args.batch` graphs of the 4096-graph sequence, solved
-    in one batched call, against looping the plain ECL-MST over the same graphs."""
+    in one batched call, against looping the plain ECL-MST over the same graphs.
+    With several ranks each solves its shard of the graphs (partitioned by CSR
+    entries, shard.py) and the time is the slowest rank's; only rank 0 reports."""
+    import shard
     t0 = time.perf_counter()
-    graphs = E.gen_batch(args.batch)
+    all_graphs = E.gen_batch(args.batch)
     gen_s = time.perf_counter() - t0
+    n_all, m_all = len(all_graphs), int(sum(g.edges for g in all_graphs))
+    graphs = all_graphs
+    if world > 1:
+        mine = shard.partition_by_cost([g.edges for g in all_graphs], world)[rank]
+        graphs = [all_graphs[i] for i in mine]
     b = E.Batch(graphs)
     total_m = int(b.edges.sum())
     ni = torch.from_numpy(b.nindex).to(dev)
@@ -205,6 +213,19 @@ def batch_leg(args, E, torch, dev):
         ms.append(last["ms_total"])
     t = sum(ms) / len(ms)
     got = out.cpu().numpy()
+    if world > 1:  # the slowest rank's time; every graph was solved by exactly one rank
+        tt = torch.tensor([t], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+        fw = {i: int(b.slice(got, k).astype(bool).sum()) for k, i in enumerate(mine)}
+        solved = shard.gather_results(fw, dist)
+        bc.close()
+        if rank != 0:
+            return None
+        return {"graphs": n_all, "edges": m_all, "ms": t, "graphs_per_s": n_all / (t * 1e-3),
+                "gedges_per_s": m_all / (t * 1e-3) / 1e9, "ranks": world, "graphs_solved": len(solved),
+                "forest_edges": sum(solved.values()), "gen_s": round(gen_s, 1),
+                "sample": f"first {n_all} graphs of the 4096-graph mixed batch, sharded by CSR entries"}
     res = {"graphs": len(graphs), "edges": total_m, "ms": t, "graphs_per_s": len(graphs) / (t * 1e-3),
            "gedges_per_s": total_m / (t * 1e-3) / 1e9, "graphs_small": last["graphs_small"],
            "graphs_large": last["graphs_large"], "cuda_graph_replay": last["graph_replay"],
@@ -494,8 +515,9 @@ def main():
                  "what": "reference ECL_MST.cu gpuMST rebuilt for sm_100a, its own timed window, median"}
 
     batch = None
-    if rank == 0 and args.batch > 0 and world == 1:
-        batch = batch_leg(args, E, torch, dev)
+    if args.batch > 0:
+        # one GPU: the whole batch; several: each rank its shard of the graphs (shard.py)
+        batch = batch_leg(args, E, torch, dev, rank, world, dist if world > 1 else None)
 
     cpu = None
     if rank == 0 and not args.no_cpu:
