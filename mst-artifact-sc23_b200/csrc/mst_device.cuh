@@ -622,10 +622,28 @@ __global__ void __launch_bounds__(kScanThreads, ScanCfg<EPT>::kMinBlocks) k_scan
 }
 
 // parent[v] = root(v) for every vertex, once before the heavy scan.
+// A per-CTA set of roots already found ends a walk as soon as it reaches one:
+// every walk through a giant light tree would otherwise read that tree's
+// root entry, one L2 line hammered by millions of threads. Roots do not
+// change during the pass (other threads only shorten paths).
 __global__ void __launch_bounds__(kThreads) k_flatten(int* parent, int n, const DevState* st) {
+  constexpr int kRootSlots = 1024;
+  __shared__ int roots[kRootSlots];
   if (!st->filtered || (ld_volatile(&st->error) & (kErrFormat | kErrTimeout))) return;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-    __stcg(parent + v, find_ro(v, parent));
+  for (int i = threadIdx.x; i < kRootSlots; i += blockDim.x) roots[i] = -1;
+  __syncthreads();
+  volatile int* known = roots;
+  auto slot = [](int x) { return ((unsigned)x * 0x85EBCA6Bu) >> 22; };  // 10 bits
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    int x = v, p = __ldcg(parent + v);
+    while (p != x) {
+      x = p;
+      if (known[slot(x)] == x) break;
+      p = __ldcg(parent + x);
+    }
+    known[slot(x)] = x;
+    if (x != v) __stcg(parent + v, x);
+  }
 }
 
 // ----------------------------------------------------------------- rounds
