@@ -31,6 +31,9 @@ struct ecl_mst_ctx {
   int sm_count = 0;
   int64_t max_nodes = 0, max_edges = 0;
   cudaStream_t stream = nullptr;
+  // the learned schedule's feature pass runs on `side`, beside k_prep
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   // [minv0 | minv1 | parent] in one allocation (one L2 access-policy window)
   void* slots = nullptr;
   int* parent = nullptr;
@@ -131,6 +134,9 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   if (!prop.cooperativeLaunch) return fail(ECL_ERR_UNSUPPORTED);
   c->sm_count = prop.multiProcessorCount;
   if ((st = cuda_status(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)))) return fail(st);
+  if ((st = cuda_status(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)))) return fail(st);
+  if ((st = cuda_status(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming)))) return fail(st);
+  if ((st = cuda_status(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming)))) return fail(st);
   const size_t slot_bytes = (size_t)max_nodes * (2 * sizeof(u64) + sizeof(int));
   if ((st = cuda_status(cudaMalloc(&c->slots, slot_bytes)))) return fail(st);
   c->minv0 = (u64*)c->slots;
@@ -181,6 +187,10 @@ extern "C" void ecl_mst_ctx_destroy(ecl_mst_ctx* c) {
   cudaFree(c->d_inMST);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
+  if (c->side) cudaStreamSynchronize(c->side);
+  if (c->fork) cudaEventDestroy(c->fork);
+  if (c->join) cudaEventDestroy(c->join);
+  if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -252,8 +262,10 @@ int launch_scans(bool device_split, int split, const ScanArgs& sa, cudaStream_t 
   return ECL_OK;
 }
 
+// `join`, when set, is recorded on the stream that runs the learned
+// schedule's feature pass; the light scan waits for it, k_prep does not.
 int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, const mst_opts* o,
-                  cudaStream_t s, bool timed) {
+                  cudaStream_t s, bool timed, cudaEvent_t join = nullptr) {
   const int n = g->nodes, m = g->edges;
   const int split = o->degree_split > 0 ? o->degree_split : kDefaultSplit;
   const bool device_split = o->threshold_mode == ECL_THRESH_LEARNED;
@@ -277,6 +289,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   const int prep_grid = (int)std::min<int64_t>((prep_items + kThreads - 1) / kThreads, (int64_t)c->sm_count * 16);
   k_prep<<<std::max(prep_grid, 1), kThreads, 0, s>>>(pa);
   ECL_CUDA_TRY(cudaGetLastError());
+  if (join) ECL_CUDA_TRY(cudaStreamWaitEvent(s, join, 0));
   ScanArgs sa;
   sa.nodes = n;
   sa.edges = m;
@@ -433,12 +446,22 @@ extern "C" int ecl_mst_run_device(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d
   // there the feature pass costs about as much as any schedule can save.
   if (o.threshold_mode == ECL_THRESH_LEARNED && g->edges < kLearnedMinEdges)
     o.threshold_mode = ECL_THRESH_HEURISTIC;
+  cudaEvent_t join = nullptr;
   if (o.threshold_mode == ECL_THRESH_LEARNED) {
-    st = ecl_learned_prepare(c, g, s, c->st);
-    if (st == ECL_ERR_UNSUPPORTED) o.threshold_mode = ECL_THRESH_HEURISTIC;  // no weights loaded
-    else if (st) return st;
+    // the feature pass and the MLP run on the side stream, beside k_prep
+    ECL_CUDA_TRY(cudaEventRecord(c->fork, s));
+    ECL_CUDA_TRY(cudaStreamWaitEvent(c->side, c->fork, 0));
+    st = ecl_learned_prepare(c, g, c->side, c->st);
+    if (st == ECL_ERR_UNSUPPORTED) {
+      o.threshold_mode = ECL_THRESH_HEURISTIC;  // no weights loaded
+    } else if (st) {
+      return st;
+    } else {
+      ECL_CUDA_TRY(cudaEventRecord(c->join, c->side));
+      join = c->join;
+    }
   }
-  if ((st = enqueue_solve(c, g, d_inMST, &o, s, stats != nullptr))) return st;
+  if ((st = enqueue_solve(c, g, d_inMST, &o, s, stats != nullptr, join))) return st;
   if (stats) {
     if (s != c->stream) {
       ECL_CUDA_TRY(cudaStreamSynchronize(s));

@@ -232,6 +232,7 @@ __global__ void k_mlp_apply(const float* p, const float* feat, const int* sorted
   }
   // output 1: log2 of the degree split, in [1, 6]
   st->learned_split = 1 << (int)lrintf(fminf(fmaxf(y[1], 1.f), 6.f));
+  st->split = st->learned_split;  // read by the scans (k_prep leaves it alone in this mode)
 }
 
 // Full-batch mean-squared-error loss and gradient of the trainable

@@ -127,17 +127,15 @@ enum : unsigned {
 // ------------------------------------------------------------------ prep
 // Threshold rule, by mode (run by one CTA). HEURISTIC restates main's rule
 // (ECL_MST.cu:408,432-440); QUANTILE takes a quantile of a 4096-entry hashed
-// sample; LEARNED keeps the threshold, filter flag and split the MLP kernel
-// already wrote into `st` (from its own sorted sample).
+// sample; LEARNED leaves the threshold, filter flag and split to the MLP
+// kernel (k_mlp_apply, which runs beside this kernel on another stream and
+// takes them from its own sorted sample).
 __device__ void choose_threshold(const PrepArgs& a, int* samp) {
   DevState* st = a.st;
   const int tid = threadIdx.x;
   int mode = a.mode, split = a.split;
   float quantile = a.quantile;
-  if (mode == ECL_THRESH_LEARNED) {
-    if (tid == 0) st->split = st->learned_split;
-    return;
-  }
+  if (mode == ECL_THRESH_LEARNED) return;
   const int nodes = a.nodes, edges = a.edges;
   if (tid == 0) st->split = split;
   if (mode == ECL_THRESH_NONE || (mode == ECL_THRESH_QUANTILE && !(quantile < 1.0f))) {
