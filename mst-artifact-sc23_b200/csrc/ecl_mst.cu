@@ -95,6 +95,26 @@ int coop_grid(const void* fn, int threads, int sm_count) {
 
 int prepare_scan_kernels();
 
+// Entries of the tile->vertex table buffer for up to `edges` CSR entries: the
+// table (tiles + 1) and the fill scan's chunk maxima.
+int64_t first_v_entries(int64_t edges) {
+  const int64_t tiles = edges / kGran + 1;
+  return tiles + 1 + tiles / kFillChunk + 1;
+}
+
+// k_prep, then the fill scan that completes the tile->vertex table
+// (first_v: pa.tiles + 1 entries, then room for the chunk maxima).
+int enqueue_prep(const PrepArgs& pa, int sm_count, cudaStream_t s) {
+  ECL_CUDA_TRY(cudaMemsetAsync(pa.first_v, 0, sizeof(int) * (size_t)pa.tiles, s));
+  const int prep_grid = (int)std::min<int64_t>((pa.nodes + kThreads - 1) / kThreads, (int64_t)sm_count * 16);
+  k_prep<<<std::max(prep_grid, 1), kThreads, 0, s>>>(pa);
+  const int chunks = (pa.tiles + kFillChunk - 1) / kFillChunk;
+  int* chunk_max = pa.first_v + pa.tiles + 1;
+  k_fill_chunks<<<chunks, 1024, 0, s>>>(pa.first_v, pa.tiles, chunk_max);
+  k_fill_carry<<<chunks, 1024, 0, s>>>(pa.first_v, pa.tiles, chunk_max, pa.nodes);
+  return cuda_status(cudaGetLastError());
+}
+
 // Round-kernel ablation bits from the option flags.
 unsigned round_ablation(int flags) {
   return ((flags & ECL_FLAG_NO_GUARDS) ? kAblNoGuards : 0u) | ((flags & ECL_FLAG_NO_WARP_COOP) ? kAblNoCoop : 0u) |
@@ -149,7 +169,7 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   c->wl_cap = (unsigned)std::max<int64_t>(max_edges + std::min<int64_t>(max_edges, kWlSlack), 1);
   for (int i = 0; i < 2; i++)
     if ((st = cuda_status(cudaMalloc(&c->wl[i], (size_t)c->wl_cap * sizeof(int4))))) return fail(st);
-  c->first_v_cap = (int)(max_edges / kGran + 2);
+  c->first_v_cap = (int)first_v_entries(max_edges);
   if ((st = cuda_status(cudaMalloc(&c->first_v, (size_t)c->first_v_cap * sizeof(int))))) return fail(st);
   if ((st = cuda_status(cudaMalloc(&c->st, sizeof(DevState))))) return fail(st);
   if ((st = cuda_status(cudaMalloc(&c->ml_params, ECL_MLP_PARAMS * sizeof(float))))) return fail(st);
@@ -285,10 +305,8 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   pa.split = split;
   pa.quantile = o->quantile;
   pa.st = c->st;
-  const int64_t prep_items = std::max<int64_t>(n, (int64_t)tiles + 1);
-  const int prep_grid = (int)std::min<int64_t>((prep_items + kThreads - 1) / kThreads, (int64_t)c->sm_count * 16);
-  k_prep<<<std::max(prep_grid, 1), kThreads, 0, s>>>(pa);
-  ECL_CUDA_TRY(cudaGetLastError());
+  int st;
+  if ((st = enqueue_prep(pa, c->sm_count, s))) return st;
   if (join) ECL_CUDA_TRY(cudaStreamWaitEvent(s, join, 0));
   ScanArgs sa;
   sa.nodes = n;
@@ -322,7 +340,6 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   ra.count_atomics = (o->flags & ECL_FLAG_STATS) ? 1 : 0;
   ra.abl = round_ablation(o->flags);
   const int rgrid = std::max(1, std::min(c->round_grid, (m / 2 + kRoundThreads - 1) / kRoundThreads + 1));
-  int st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[5], s));
   if ((st = launch_scans<kLight>(device_split, split, sa, s))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[1], s));
@@ -548,7 +565,8 @@ namespace {
 constexpr int64_t kNaMaxNodes = 1 << 18;              // 262,144 vertices
 constexpr int64_t kNaMaxEdges = 1 << 20;              // 1,048,576 directed CSR entries
 constexpr int64_t kNaWlCap = kNaMaxEdges / 2;         // one-direction entries per worklist
-constexpr int64_t kNaTiles = kNaMaxEdges / kGran + 2; // tile -> vertex table entries
+// tile -> vertex table entries, with the fill scan's chunk maxima
+constexpr int64_t kNaTiles = kNaMaxEdges / kGran + 2 + (kNaMaxEdges / kGran + 1) / kFillChunk + 1;
 
 constexpr size_t na_align(size_t x) { return (x + 255) & ~(size_t)255; }
 constexpr size_t kNaOffState = 0;
@@ -647,10 +665,7 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   pa.split = split;
   pa.quantile = o.quantile;
   pa.st = dst;
-  const int64_t prep_items = std::max<int64_t>(n, (int64_t)tiles + 1);
-  const int prep_grid = (int)std::min<int64_t>((prep_items + kThreads - 1) / kThreads, (int64_t)d->sm_count * 16);
-  k_prep<<<std::max(prep_grid, 1), kThreads, 0, s>>>(pa);
-  ECL_CUDA_TRY(cudaGetLastError());
+  if ((st = enqueue_prep(pa, d->sm_count, s))) return st;
   ScanArgs sa;
   sa.nodes = n;
   sa.edges = m;

@@ -212,17 +212,6 @@ __device__ void choose_threshold(const PrepArgs& a, int* samp) {
   }
 }
 
-// Largest v in [0, nodes) with nindex[v] <= e (bounded even on bad input).
-__device__ __forceinline__ int vertex_of(const int* nindex, int nodes, long long e) {
-  int lo = 0, hi = nodes;  // invariant: nindex[lo] <= e (for a valid CSR), answer in [lo, hi)
-  while (hi - lo > 1) {
-    const int mid = lo + ((hi - lo) >> 1);
-    if ((long long)__ldg(nindex + mid) <= e) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
-
 __global__ void __launch_bounds__(kThreads) k_prep(PrepArgs a) {
   __shared__ int samp[4096];
   DevState* st = a.st;
@@ -235,12 +224,79 @@ __global__ void __launch_bounds__(kThreads) k_prep(PrepArgs a) {
     a.minv0[v] = kNoEdge;
     a.minv1[v] = kNoEdge;
     const int b = __ldg(a.nindex + v), e = __ldg(a.nindex + v + 1);
-    bad |= b < 0 || e < b || e > m;
+    const bool row_bad = b < 0 || e < b || e > m;
+    bad |= row_bad;
+    // Tile->vertex table (first_v[t] = row of entry t * kGran), first step:
+    // the row holding the first step position at or after its start writes
+    // itself there (each position has exactly one owner, so no conflicts);
+    // the positions further inside long rows stay 0 and are filled by a max
+    // scan (k_fill_chunks, k_fill_carry), rows being in increasing order.
+    const unsigned t0 = ((unsigned)b + kGran - 1) / kGran, t1 = ((unsigned)e + kGran - 1) / kGran;
+    if (!row_bad && t0 < t1) a.first_v[t0] = v;
   }
   if (gid == 0) bad |= __ldg(a.nindex) != 0 || __ldg(a.nindex + n) != m;
   if (bad) atomicOr(&st->error, kErrFormat);
-  for (int t = gid; t <= a.tiles; t += stride)
-    a.first_v[t] = t < a.tiles ? vertex_of(a.nindex, n, (long long)t * kGran) : n - 1;
+}
+
+// Inclusive max scan of the tile->vertex table first_v[0 .. tiles), in
+// chunks of kFillChunk entries: each CTA scans its chunk and records the
+// chunk's maximum; k_fill_carry then raises every chunk to the maximum of the
+// chunks before it and writes the end sentinel first_v[tiles] = nodes - 1.
+constexpr int kFillChunk = 8192;  // 1024 threads x 8 entries
+
+__global__ void __launch_bounds__(1024) k_fill_chunks(int* t, int count, int* chunk_max) {
+  __shared__ int warp_max[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long base = (long long)blockIdx.x * kFillChunk + threadIdx.x * 8;
+  int x[8], run = 0;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    x[q] = base + q < count ? t[base + q] : 0;
+    run = max(run, x[q]);
+    x[q] = run;
+  }
+  int incl = run;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl = max(incl, y);
+  }
+  if (lane == 31) warp_max[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int w = warp_max[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w = max(w, y);
+    }
+    warp_max[lane] = w;
+  }
+  __syncthreads();
+  int before = __shfl_up_sync(0xffffffffu, incl, 1);
+  if (lane == 0) before = 0;
+  if (warp > 0) before = max(before, warp_max[warp - 1]);
+#pragma unroll
+  for (int q = 0; q < 8; q++)
+    if (base + q < count) t[base + q] = max(x[q], before);
+  if (threadIdx.x == 0) chunk_max[blockIdx.x] = warp_max[31];
+}
+
+__global__ void __launch_bounds__(1024) k_fill_carry(int* t, int count, const int* chunk_max, int nodes) {
+  __shared__ int carry;
+  if (threadIdx.x < 32) {
+    int c = 0;
+    for (int i = threadIdx.x; i < (int)blockIdx.x; i += 32) c = max(c, chunk_max[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c = max(c, __shfl_xor_sync(0xffffffffu, c, o));
+    if (threadIdx.x == 0) carry = c;
+  }
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * kFillChunk;
+  if (carry > 0)
+    for (int q = threadIdx.x; q < kFillChunk && base + q < count; q += blockDim.x)
+      t[base + q] = max(t[base + q], carry);
+  if (blockIdx.x == 0 && threadIdx.x == 0) t[count] = nodes - 1;
 }
 
 // ------------------------------------------------------------------ scans
