@@ -370,14 +370,24 @@ def main():
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             flush.max()  # L2 flush between timed iterations (outside the timed events)
-            st = solve(True)  # CUDA events around the solve on `stream`; syncs after
+            # CUDA events around the solve on `stream` (a repeated solve is replayed
+            # from its captured CUDA graph); syncs after
+            st = solve(True)
             step_ms.append(st["ms_total"])
+        torch.cuda.synchronize()
+    # per-kernel breakdown (roofline): the same solve with direct launches and
+    # events between the phases
+    bd_opts = E.make_opts(mode=mode, quantile=args.quantile, degree_split=args.split, flags=E.FLAG_NO_GRAPH)
+    for i in range(2 + max(3, args.steps // 5)):
+        flush.max()
+        st = ctx.run_device(g.nodes, g.edges, d_ni.data_ptr(), d_nl.data_ptr(), d_ew.data_ptr(),
+                            d_out.data_ptr(), opts=bd_opts, stream=stream.cuda_stream, stats=True)
+        if i >= 2:
             scan_ms.append(st["ms_scan"])
             round_ms.append(st["ms_rounds"])
             light_us.append(st["us_scan"][0][2])
             heavy_us.append(st["us_scan"][1][2])
             last = st
-        torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     clocks = clk.summary()

@@ -143,7 +143,12 @@ enum {
   ECL_FLAG_DEDUP = 1 << 5,         /* per-tile parallel-edge elimination in the
                                       rounds (off by default: on RMAT it costs
                                       more than the smaller worklists save)     */
-  ECL_FLAG_NO_FIND_CACHE = 1 << 6  /* no per-CTA root cache in the finds        */
+  ECL_FLAG_NO_FIND_CACHE = 1 << 6, /* no per-CTA root cache in the finds        */
+  /* A solve repeated with identical arguments is captured as a CUDA graph on
+   * the first repeat and replayed as one launch after that; a replayed
+   * solve's stats carry ms_total only. NO_GRAPH keeps direct launches (and
+   * the per-phase timings). */
+  ECL_FLAG_NO_GRAPH = 1 << 7
 };
 
 typedef struct mst_opts {

@@ -352,6 +352,13 @@ extern "C" int ecl_learned_has_weights(void) {
   return g_weights.empty() ? 0 : 1;
 }
 
+// Version of the loaded weights (bumped by every load); part of the key of a
+// captured solve, whose graph does not re-upload them.
+unsigned ecl_learned_weights_version() {
+  std::lock_guard<std::mutex> lock(g_w_mu);
+  return g_w_version;
+}
+
 // Features + MLP on the device for the learned schedule; writes the decoded
 // quantile and split into the solve's control block. Returns
 // ECL_ERR_UNSUPPORTED when no weights are loaded (the caller then falls back

@@ -31,6 +31,8 @@ THRESH_HEURISTIC, THRESH_NONE, THRESH_EXPLICIT, THRESH_QUANTILE, THRESH_LEARNED 
 FLAG_L2_PERSIST, FLAG_STATS, FLAG_NO_SMALL_TAIL = 1, 2, 4
 # ablation switches (the answer is unchanged; see include/ecl_mst.h)
 FLAG_NO_GUARDS, FLAG_NO_WARP_COOP, FLAG_DEDUP, FLAG_NO_FIND_CACHE = 8, 16, 32, 64
+# direct launches instead of replaying a captured solve (keeps per-phase timings)
+FLAG_NO_GRAPH = 128
 MAX_ROUNDS = 64
 
 

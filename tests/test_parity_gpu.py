@@ -302,3 +302,29 @@ def test_cli_variants_and_table_pipeline(tmp_path):
     assert len(inputs) == 1 and all(x is not None and x > 0 for x in tp[0])
     r = subprocess.run([exe, path, "3", "NAG_NW_NF_NIPC"], capture_output=True, text=True, timeout=60)
     assert r.returncode != 0
+
+
+def test_repeated_solve_is_captured_and_replayed(ctx):
+    """A solve repeated on the same buffers and options is captured as a CUDA
+    graph on the first repeat and replayed after that; the replay reads the
+    buffers afresh, so changed weights give the new forest."""
+    import torch
+    g = E.gen_rmat(16, 16, 0.57, 0.19, 0.19, 12, 1 << 20)
+    dev = torch.device("cuda:0")
+    ni = torch.from_numpy(g.nindex).to(dev)
+    nl = torch.from_numpy(g.nlist).to(dev)
+    ew = torch.from_numpy(g.eweight).to(dev)
+    out = torch.empty(g.edges, dtype=torch.uint8, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    E.learned_load_default()
+    for kw in (dict(), dict(mode=E.THRESH_LEARNED)):
+        o = E.make_opts(**kw)
+        for step in range(4):
+            w = g.eweight if step < 3 else (g.eweight ^ 0x5A5A).astype(np.int32)
+            ew.copy_(torch.from_numpy(w))
+            out.fill_(7)
+            st = ctx.run_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(),
+                                opts=o, stream=s, stats=True)
+            want, _, _ = O.oracle_mst(g.nindex, g.nlist, w, st["threshold"], st["filtered"])
+            assert np.array_equal(out.cpu().numpy(), want), (kw, step)
+            assert st["ms_total"] > 0 and st["status"] == 0
