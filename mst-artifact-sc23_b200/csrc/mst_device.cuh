@@ -50,7 +50,10 @@ constexpr int kGran = 128;             // entries per tile->vertex table step (t
 #define ECL_PAIR_LOG 10
 #endif
 constexpr int kRoundThreads = ECL_ROUND_THREADS;  // threads of a round CTA (one worklist entry each per tile)
-constexpr int kEPT = 1;                // worklist entries per thread in a round tile
+#ifndef ECL_ROUND_EPT
+#define ECL_ROUND_EPT 1
+#endif
+constexpr int kEPT = ECL_ROUND_EPT;    // worklist entries per thread in a round tile
 constexpr int kHotLog = 9;             // hot representative table: 512 slots
 constexpr int kHotSlots = 1 << kHotLog;
 constexpr int kFindLog = ECL_FIND_LOG; // find cache
