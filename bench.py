@@ -182,34 +182,48 @@ def batch_leg(args, E, torch, dev, rank=0, world=1, dist=None):
     [1e3, 2e6] vertices; grid / ER deg 8 / RMAT ef 8 / RGG2D deg 3; weights
     U[1, 2^20]): the first `args.batch` graphs of the 4096-graph sequence, solved
     in one batched call, against looping the plain ECL-MST over the same graphs.
-    With several ranks each solves its shard of the graphs (partitioned by CSR
-    entries, shard.py) and the time is the slowest rank's; only rank 0 reports."""
+    The graphs are drawn by the host generators, or with --batch-gen device by
+    the device generators straight into the packed device layout (the same
+    graphs; no host copy of the batch exists then). With several ranks each
+    solves its shard of the graphs (partitioned by CSR entries, shard.py) and
+    the time is the slowest rank's; only rank 0 reports."""
     import shard
     t0 = time.perf_counter()
-    all_graphs = E.gen_batch(args.batch)
-    gen_s = time.perf_counter() - t0
-    n_all, m_all = len(all_graphs), int(sum(g.edges for g in all_graphs))
-    graphs = all_graphs
-    if world > 1:
-        mine = shard.partition_by_cost([g.edges for g in all_graphs], world)[rank]
-        graphs = [all_graphs[i] for i in mine]
-    b = E.Batch(graphs)
-    total_m = int(b.edges.sum())
-    ni = torch.from_numpy(b.nindex).to(dev)
-    nl = torch.from_numpy(b.nlist).to(dev)
-    ew = torch.from_numpy(b.eweight).to(dev)
+    on_device = args.batch_gen == "device" and world == 1
+    if on_device:
+        b = E.DeviceBatch(args.batch)
+        gen_s = time.perf_counter() - t0
+        n_all, m_all = b.num_graphs, int(b.edges.astype(np.int64).sum())
+        get_graph = b.graph
+        d_ni, d_nl, d_ew = b.d_nindex, b.d_nlist, b.d_eweight
+    else:
+        all_graphs = E.gen_batch(args.batch)
+        gen_s = time.perf_counter() - t0
+        n_all, m_all = len(all_graphs), int(sum(g.edges for g in all_graphs))
+        graphs = all_graphs
+        if world > 1:
+            mine = shard.partition_by_cost([g.edges for g in all_graphs], world)[rank]
+            graphs = [all_graphs[i] for i in mine]
+        b = E.Batch(graphs)
+        get_graph = graphs.__getitem__
+        ni = torch.from_numpy(b.nindex).to(dev)
+        nl = torch.from_numpy(b.nlist).to(dev)
+        ew = torch.from_numpy(b.eweight).to(dev)
+        d_ni, d_nl, d_ew = ni.data_ptr(), nl.data_ptr(), ew.data_ptr()
+    count = b.num_graphs
+    total_m = int(b.edges.astype(np.int64).sum())
     out = torch.zeros(b.total_edges, dtype=torch.uint8, device=dev)
     flush = torch.zeros(256 << 20, dtype=torch.uint8, device=dev)
-    bc = E.BatchContext(len(graphs), int(b.nodes.max()), int(b.edges.max()), 1 << 21)
+    bc = E.BatchContext(count, int(b.nodes.max()), int(b.edges.max()), 1 << 21)
     stream = torch.cuda.current_stream(dev).cuda_stream
-    best, tune_ms = bc.autotune(b, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr())
+    best, tune_ms = bc.autotune(b, d_ni, d_nl, d_ew, out.data_ptr())
     for _ in range(2):
-        bc.run(b, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(), opts=best, stream=stream)
+        bc.run(b, d_ni, d_nl, d_ew, out.data_ptr(), opts=best, stream=stream)
     ms = []
     last = None
     for _ in range(max(3, args.steps // 2)):
         flush.max()
-        last = bc.run(b, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(), opts=best, stream=stream)
+        last = bc.run(b, d_ni, d_nl, d_ew, out.data_ptr(), opts=best, stream=stream)
         ms.append(last["ms_total"])
     t = sum(ms) / len(ms)
     got = out.cpu().numpy()
@@ -226,14 +240,15 @@ def batch_leg(args, E, torch, dev, rank=0, world=1, dist=None):
                 "gedges_per_s": m_all / (t * 1e-3) / 1e9, "ranks": world, "graphs_solved": len(solved),
                 "forest_edges": sum(solved.values()), "gen_s": round(gen_s, 1),
                 "sample": f"first {n_all} graphs of the 4096-graph mixed batch, sharded by CSR entries"}
-    res = {"graphs": len(graphs), "edges": total_m, "ms": t, "graphs_per_s": len(graphs) / (t * 1e-3),
+    res = {"graphs": count, "edges": total_m, "ms": t, "graphs_per_s": count / (t * 1e-3),
            "gedges_per_s": total_m / (t * 1e-3) / 1e9, "graphs_small": last["graphs_small"],
            "graphs_large": last["graphs_large"], "cuda_graph_replay": last["graph_replay"],
            "ms_small": last["ms_small"], "ms_large": last["ms_large"],
            "autotuned": {"batch_small_edges": best.batch_small_edges, "degree_split": best.degree_split,
                          "small_tail": best.small_tail},
-           "gen_s": round(gen_s, 1),
-           "sample": f"first {len(graphs)} graphs of the 4096-graph mixed batch (seeds 1000..{999 + len(graphs)})"}
+           "generated_on": "device" if on_device else "host", "gen_s": round(gen_s, 1),
+           "sample": (f"the whole 4096-graph mixed batch" if count == 4096 else
+                      f"first {count} graphs of the 4096-graph mixed batch (seeds 1000..{999 + count})")}
     plain_so = os.path.join(ROOT, "baseline", "_ref", "libecl_plain.so")
     if os.path.exists(plain_so) and not args.no_plain:
         import ctypes
@@ -241,7 +256,8 @@ def batch_leg(args, E, torch, dev, rank=0, world=1, dist=None):
         P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
         tot = 0.0
         same = True
-        for gi, g in enumerate(graphs):
+        for gi in range(count):
+            g = get_graph(gi)
             if g.edges == 0:
                 continue
             f, th = ctypes.c_int(), ctypes.c_int()
@@ -252,12 +268,48 @@ def batch_leg(args, E, torch, dev, rank=0, world=1, dist=None):
                               ctypes.byref(s))
             tot += s.value
             same &= bool(np.array_equal(pout, b.slice(got, gi)))
-        res["plain"] = {"ms": tot * 1e3, "graphs_per_s": len(graphs) / tot, "gedges_per_s": total_m / tot / 1e9,
+        res["plain"] = {"ms": tot * 1e3, "graphs_per_s": count / tot, "gedges_per_s": total_m / tot / 1e9,
                         "inMST_identical": same,
                         "what": "reference gpuMST rebuilt for sm_100a, looped over the graphs, sum of its own timed windows"}
         res["vs_plain_graphs_per_s"] = res["graphs_per_s"] / res["plain"]["graphs_per_s"]
     bc.close()
+    if on_device:
+        b.close()
     return res
+
+
+def device_graph(E, kind, kw):
+    """The workload drawn by the device generators (identical to make_graph's)."""
+    if kind == "rmat":
+        return E.gen_rmat_device(kw["scale"], kw["edge_factor"], RMAT["a"], RMAT["b"], RMAT["c"], kw["seed"],
+                                 kw["wmax"])
+    if kind == "grid":
+        return E.gen_grid_device(kw["rows"], kw["cols"], kw["seed"], kw["wmax"])
+    if kind == "er":
+        return E.gen_er_device(kw["nodes"], kw["avg_degree"], kw["seed"], kw["wmax"])
+    raise ValueError(kind)
+
+
+def preprocess_leg(E, kind, kw, g, gen_s):
+    """GPU-side preprocessing: the workload's graph drawn on the device (pair
+    sampling, radix sort of both directions, dedup, CSR emit) against the host
+    generator on all host cores; the two graphs must be identical."""
+    ms = []
+    dg = None
+    for _ in range(3):
+        if dg is not None:
+            dg.close()
+        t0 = time.perf_counter()
+        dg = device_graph(E, kind, kw)
+        ms.append((time.perf_counter() - t0) * 1e3)
+    h = dg.to_host()
+    dg.close()
+    same = bool(np.array_equal(h.nindex, g.nindex) and np.array_equal(h.nlist, g.nlist)
+                and np.array_equal(h.eweight, g.eweight))
+    best = min(ms[1:])
+    return {"device_gen_ms": best, "host_gen_ms": gen_s * 1e3, "speedup": gen_s * 1e3 / best,
+            "host_threads": os.cpu_count(), "identical": same,
+            "what": "synchronous ecl_gen_*_device call (wall clock, outputs cudaMalloc'd) vs the host generator"}
 
 
 def reference_arm(args, E):
@@ -307,6 +359,8 @@ def main():
     ap.add_argument("--no-ablation", action="store_true", help="skip the technique-ablation leg")
     ap.add_argument("--batch", type=int, default=256,
                     help="graphs of the mixed batch to solve in batched mode (0 = skip)")
+    ap.add_argument("--batch-gen", choices=["host", "device"], default="host",
+                    help="draw the batch with the host generators or on the device (same graphs)")
     ap.add_argument("--profile", action="store_true",
                     help="device solves only (no e2e, plain or CPU legs): the command profiled by ncu")
     args = ap.parse_args()
@@ -334,6 +388,10 @@ def main():
     t0 = time.perf_counter()
     g = make_graph(E, kind, kw)
     gen_s = time.perf_counter() - t0
+
+    preprocess = None
+    if rank == 0 and not args.profile:
+        preprocess = preprocess_leg(E, kind, kw, g, gen_s)
 
     have_weights = E.learned_load_default()
     if args.mode == "learned" and not have_weights:
@@ -557,9 +615,10 @@ def main():
                        "ms_median": statistics.median(step_ms), "gen_s": round(gen_s, 2)},
             "e2e": {"value": world * g.edges / e2e_mean / 1e9, "unit": "Gedges/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms": e2e_mean * 1e3},
-            # per solve: k_prep, k_scan x2, k_rounds x2, k_flatten; the learned schedule adds
-            # k_feat_degrees, k_feat_finish, k_mlp_apply and launches all three scan variants
-            "gpu_launches": (13 if args.mode == "learned" else 6) * args.steps,
+            # per solve: k_prep, k_fill_chunks, k_fill_carry, k_scan x2, k_rounds x2, k_flatten; the
+            # learned schedule adds k_feat_degrees, k_feat_finish, k_mlp_apply and launches all
+            # three scan variants per phase (the two not selected exit at once)
+            "gpu_launches": (15 if args.mode == "learned" else 8) * args.steps,
             "ablation": ablation,
             "heuristic_schedule": ({"value": world * g.edges / (np.mean(heur_ms) * 1e-3) / 1e9,
                                     "ms": float(np.mean(heur_ms)),
@@ -569,6 +628,7 @@ def main():
             "cpu_baseline": cpu,
             "plain_ecl_mst": plain,
             "batch": batch,
+            "preprocess": preprocess,
             "vs_plain": (value / plain["value"]) if plain else None,
             "forest_weight": fw,
             "clocks": clocks,

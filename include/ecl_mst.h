@@ -112,6 +112,63 @@ int ecl_gen_rgg2d(int32_t nodes, double avg_degree, uint64_t seed,
 int ecl_gen_batch_graph(int32_t index, uint64_t seed0, int32_t nmin, int32_t nmax,
                         int32_t wmax, ecl_graph* out, int32_t* family);
 
+/* ------------------------------------------------ GPU-side preprocessing */
+/* The reference builds and converts its inputs on the host
+ * (Inputs/download_inputs.sh, PBBS_CPU/inputs/ecl2pbbs_genweights.cpp:14-41,
+ * cuGraph_GPU/inputs/ecl2mtx_genweights_cugraph.cpp:16-50). These build them
+ * on the device. Every call is synchronous; on success the ecl_graph holds
+ * DEVICE arrays from cudaMalloc, freed with ecl_free_device_graph. */
+
+/* Weight of each CSR entry built by ecl_csr_from_pairs_device. */
+typedef enum ecl_weight_rule {
+  ECL_WEIGHTS_GIVEN = 0, /* d_w[i] of the pair; duplicates of an undirected
+                            pair keep the smallest as uint32 (the MST order) */
+  ECL_WEIGHTS_HASH = 1,  /* the generators' rule: uniform in [1, wmax] from a
+                            hash of (seed, min(u,v), max(u,v))               */
+  ECL_WEIGHTS_SYNTH = 2  /* the reference's weight for weightless inputs,
+                            1 + ((u*v) % nodes) made non-negative
+                            (ECL_MST.cu:410-419)                            */
+} ecl_weight_rule;
+
+/* Symmetric, deduplicated, self-loop-free CSR with rows sorted by neighbour
+ * id, from `pairs` undirected pairs (d_u[i], d_v[i]) in DEVICE memory (either
+ * orientation; duplicates and self-loops allowed). An id outside
+ * [0, nodes) gives ECL_ERR_FORMAT; 2 * pairs > INT32_MAX gives
+ * ECL_ERR_TOO_LARGE. stream NULL = the default stream. */
+int ecl_csr_from_pairs_device(int32_t nodes, int64_t pairs, const int32_t* d_u,
+                              const int32_t* d_v, const int32_t* d_w,
+                              int32_t weight_rule, uint64_t seed, int32_t wmax,
+                              void* stream, ecl_graph* out);
+
+/* The synthetic families drawn on the device: for equal arguments the result
+ * equals the host generator's (ecl_gen_grid, ...) entry for entry. */
+int ecl_gen_grid_device(int32_t rows, int32_t cols, uint64_t seed, int32_t wmax,
+                        void* stream, ecl_graph* out);
+int ecl_gen_er_device(int32_t nodes, double avg_degree, uint64_t seed,
+                      int32_t wmax, void* stream, ecl_graph* out);
+int ecl_gen_rmat_device(int32_t scale, int32_t edge_factor, double a, double b,
+                        double c, uint64_t seed, int32_t wmax, void* stream,
+                        ecl_graph* out);
+int ecl_gen_rgg2d_device(int32_t nodes, double avg_degree, uint64_t seed,
+                         int32_t wmax, void* stream, ecl_graph* out);
+int ecl_gen_batch_graph_device(int32_t index, uint64_t seed0, int32_t nmin,
+                               int32_t nmax, int32_t wmax, void* stream,
+                               ecl_graph* out, int32_t* family);
+void ecl_free_device_graph(ecl_graph* g);
+
+/* Copy a device graph into malloc'd host arrays (free with ecl_free_graph). */
+int ecl_graph_to_host(const ecl_graph* d_graph, ecl_graph* out);
+
+/* ------------------------------------------------------------- exporters */
+/* Text formats of the reference's converters, byte for byte. Weightless
+ * graphs (eweight NULL) get the ECL_WEIGHTS_SYNTH weights, as there.
+ *   PBBS WeightedEdgeArray: every CSR entry as "src dst weight" with the
+ *     weight printed as float with %f (ecl2pbbs_genweights.cpp:34-41);
+ *   MatrixMarket coordinate real symmetric: the entries with src > dst,
+ *     1-based, weight with %.1f (ecl2mtx_genweights_cugraph.cpp:37-50). */
+int ecl_write_pbbs(const ecl_graph* g, const char* path);
+int ecl_write_mtx(const ecl_graph* g, const char* path);
+
 /* ------------------------------------------------------------- threshold */
 typedef enum ecl_threshold_mode {
   ECL_THRESH_HEURISTIC = 0, /* the reference rule (ECL_MST.cu:408,432-444)      */
@@ -306,6 +363,19 @@ int ecl_mst_run_batch_device(ecl_batch_ctx* ctx, const ecl_batch* batch,
  * every candidate; only the time differs. */
 int ecl_batch_autotune(ecl_batch_ctx* ctx, const ecl_batch* batch, uint8_t* d_inMST,
                        const mst_opts* base, mst_opts* best, float* best_ms);
+
+/* The first `count` graphs of the mixed batch (ecl_gen_batch_graph's
+ * sequence), drawn on the device and packed into one ecl_batch whose segments
+ * start at multiples of `align` entries (nindex: nodes + 1 entries per graph,
+ * nlist/eweight: max(edges, 1)). Graph g's inMST segment of a solve is
+ * [edge_off[g], edge_off[g] + edges[g]); the packed length is
+ * edge_off[count-1] + round_up(max(edges[count-1], 1), align). The host arrays
+ * are malloc'd, the device arrays cudaMalloc'd; free both with
+ * ecl_free_device_batch. family (count entries) may be NULL. Synchronous. */
+int ecl_gen_batch_device(int32_t count, uint64_t seed0, int32_t nmin, int32_t nmax,
+                         int32_t wmax, int32_t align, void* stream, ecl_batch* out,
+                         int32_t* family);
+void ecl_free_device_batch(ecl_batch* b);
 
 /* ---------------------------------------------------- learned schedule */
 /* A 16 -> 64 -> 64 -> 2 ReLU MLP (fp32) maps 16 graph features to the light-

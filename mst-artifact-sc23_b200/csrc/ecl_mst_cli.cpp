@@ -13,6 +13,10 @@
 // atomic guards, the warp cooperation and the filter of this engine (the
 // forest is unchanged). The reference's later steps (NIPC, NOD, NT, NDD,
 // NEB) remove structure this engine is built on and are not reproduced.
+//
+// ecl_mst --to-pbbs|--to-mtx <graph.egr> <out> converts a graph for the other
+// MST codes of the artifact, as PBBS_CPU/inputs/ecl2pbbs_genweights.cpp and
+// cuGraph_GPU/inputs/ecl2mtx_genweights_cugraph.cpp do (same file bytes).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -39,9 +43,30 @@ static bool variant_opts(const char* name, mst_opts* o) {
   return true;
 }
 
+static int convert(const char* mode, const char* in, const char* out) {
+  ecl_graph g;
+  int st = ecl_read_graph(in, &g);
+  if (st) {
+    fprintf(stderr, "ERROR: %s: %s\n", in, ecl_status_string(st));
+    return 1;
+  }
+  printf("input: %s\nnodes: %d\nedges: %d\nweights: %s\n", in, g.nodes, g.edges,
+         g.eweight ? "from file" : "synthesised");
+  st = strcmp(mode, "--to-pbbs") == 0 ? ecl_write_pbbs(&g, out) : ecl_write_mtx(&g, out);
+  ecl_free_graph(&g);
+  if (st) {
+    fprintf(stderr, "ERROR: %s: %s\n", out, ecl_status_string(st));
+    return 1;
+  }
+  return 0;
+}
+
 int main(int argc, char* argv[]) {
-  if (argc < 2 || argc > 4) {
-    printf("USAGE: %s input_graph [runs] [variant: base | NAG | NAG_NW | NAG_NW_NF]\n", argv[0]);
+  if (argc == 4 && (strcmp(argv[1], "--to-pbbs") == 0 || strcmp(argv[1], "--to-mtx") == 0))
+    return convert(argv[1], argv[2], argv[3]);
+  if (argc < 2 || argc > 4 || argv[1][0] == '-') {
+    printf("USAGE: %s input_graph [runs] [variant: base | NAG | NAG_NW | NAG_NW_NF]\n"
+           "       %s --to-pbbs | --to-mtx input_graph output_file\n", argv[0], argv[0]);
     return 1;
   }
   const int runs = argc >= 3 ? atoi(argv[2]) : 9;

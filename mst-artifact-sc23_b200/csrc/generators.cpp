@@ -109,6 +109,47 @@ int build_csr(int32_t n, const std::vector<uint64_t>& pairs, uint64_t seed, int3
 
 }  // namespace
 
+EclRmatCut ecl_rmat_cut(double a, double b, double c) {
+  EclRmatCut cut;
+  cut.ta = (uint32_t)std::lround(a * 65536.0);
+  cut.tab = (uint32_t)std::lround((a + b) * 65536.0);
+  cut.tabc = (uint32_t)std::lround((a + b + c) * 65536.0);
+  return cut;
+}
+
+EclRggGrid ecl_rgg_grid(int32_t nodes, double avg_degree) {
+  // Unit square in 31-bit fixed point; radius from E[deg] = n * pi * r^2.
+  const double kOne = 2147483648.0;
+  const double rad = std::sqrt(avg_degree / (M_PI * (double)nodes));
+  const uint64_t r_fix = (uint64_t)std::min(kOne, std::floor(rad * kOne));
+  EclRggGrid g;
+  g.r2 = r_fix * r_fix;
+  // Cells at least one radius wide, and no more than about 4n of them.
+  const int64_t cap = 2 * (int64_t)std::sqrt((double)nodes) + 1;
+  g.cells = std::max<int64_t>(1, std::min<int64_t>(cap, (int64_t)(kOne / std::max<uint64_t>(r_fix, 1))));
+  g.cell_w = (uint64_t)std::ceil(kOne / (double)g.cells);
+  return g;
+}
+
+// Graph `index` of the mixed batch: seed = seed0 + index; the family is
+// uniform over {grid, Erdos-Renyi (avg degree 8), RMAT (0.57, 0.19, 0.19,
+// edge factor 8), random geometric 2D (avg degree 3)} and the vertex count
+// log-uniform in [nmin, nmax] (RMAT rounds it to a power of two, the grid to
+// rows x cols with rows = floor(sqrt(n))).
+EclBatchPick ecl_batch_pick(int32_t index, uint64_t seed0, int32_t nmin, int32_t nmax) {
+  EclBatchPick p;
+  p.seed = seed0 + (uint64_t)index;
+  const uint64_t r0 = ecl_rng(p.seed, 5, 0), r1 = ecl_rng(p.seed, 5, 1);
+  p.family = (int)(r0 % 4);
+  const double u = (double)(r1 >> 11) * (1.0 / 9007199254740992.0);
+  const double ln = std::log((double)nmin) + u * (std::log((double)nmax) - std::log((double)nmin));
+  p.nodes = (int32_t)std::max<double>(nmin, std::min<double>(nmax, std::llround(std::exp(ln))));
+  p.rows_or_scale = 0;
+  if (p.family == 0) p.rows_or_scale = std::max<int32_t>(1, (int32_t)std::sqrt((double)p.nodes));
+  if (p.family == 2) p.rows_or_scale = std::max<int32_t>(1, (int32_t)std::lround(std::log2((double)p.nodes)));
+  return p;
+}
+
 extern "C" int ecl_gen_grid(int32_t rows, int32_t cols, uint64_t seed, int32_t wmax, int threads,
                             ecl_graph* out) {
   if (!out || rows < 1 || cols < 1 || wmax < 1) return ECL_ERR_INVALID_ARG;
@@ -179,11 +220,9 @@ extern "C" int ecl_gen_rmat(int32_t scale, int32_t edge_factor, double a, double
   const int32_t n = 1 << scale;
   const int64_t samples = (int64_t)edge_factor << scale;
   if (2 * samples > INT32_MAX) return ECL_ERR_TOO_LARGE;
-  // Quadrant thresholds in 16-bit fixed point: each recursion level consumes
-  // 16 random bits, four levels per 64-bit draw.
-  const uint32_t ta = (uint32_t)std::lround(a * 65536.0);
-  const uint32_t tab = (uint32_t)std::lround((a + b) * 65536.0);
-  const uint32_t tabc = (uint32_t)std::lround((a + b + c) * 65536.0);
+  // Each recursion level consumes 16 random bits, four levels per 64-bit draw.
+  const EclRmatCut cut = ecl_rmat_cut(a, b, c);
+  const uint32_t ta = cut.ta, tab = cut.tab, tabc = cut.tabc;
   std::vector<uint64_t> pairs((size_t)samples);
   parallel_for(samples, threads, [&](int64_t bb, int64_t e, int) {
     for (int64_t i = bb; i < e; i++) {
@@ -206,15 +245,9 @@ extern "C" int ecl_gen_rgg2d(int32_t nodes, double avg_degree, uint64_t seed, in
                              int threads, ecl_graph* out) {
   if (!out || nodes < 1 || avg_degree < 0 || wmax < 1) return ECL_ERR_INVALID_ARG;
   threads = resolve_threads(threads);
-  // Unit square in 31-bit fixed point; radius from E[deg] = n * pi * r^2.
-  const double kOne = 2147483648.0;
-  const double rad = std::sqrt(avg_degree / (M_PI * (double)nodes));
-  const uint64_t r_fix = (uint64_t)std::min(kOne, std::floor(rad * kOne));
-  const uint64_t r2 = r_fix * r_fix;
-  // Cells at least one radius wide, and no more than about 4n of them.
-  const int64_t cap = 2 * (int64_t)std::sqrt((double)nodes) + 1;
-  const int64_t cells = std::max<int64_t>(1, std::min<int64_t>(cap, (int64_t)(kOne / std::max<uint64_t>(r_fix, 1))));
-  const uint64_t cell_w = (uint64_t)std::ceil(kOne / (double)cells);
+  const EclRggGrid grid = ecl_rgg_grid(nodes, avg_degree);
+  const uint64_t r2 = grid.r2, cell_w = grid.cell_w;
+  const int64_t cells = grid.cells;
   std::vector<uint32_t> px(nodes), py(nodes);
   std::vector<uint64_t> order(nodes);
   parallel_for(nodes, threads, [&](int64_t b, int64_t e, int) {
@@ -272,34 +305,24 @@ extern "C" int ecl_gen_rgg2d(int32_t nodes, double avg_degree, uint64_t seed, in
   return build_csr(nodes, pairs, seed, wmax, threads, out);
 }
 
-// Graph `index` of the mixed batch: seed = seed0 + index; the family is
-// uniform over {grid, Erdos-Renyi (avg degree 8), RMAT (0.57, 0.19, 0.19,
-// edge factor 8), random geometric 2D (avg degree 3)} and the vertex count
-// log-uniform in [nmin, nmax] (RMAT rounds it to a power of two, the grid to
-// rows x cols with rows = floor(sqrt(n))). Single-threaded, so many graphs
-// can be generated in parallel.
+// Graph `index` of the mixed batch (family, size and seed from
+// ecl_batch_pick). Single-threaded, so many graphs can be generated in
+// parallel.
 extern "C" int ecl_gen_batch_graph(int32_t index, uint64_t seed0, int32_t nmin, int32_t nmax,
                                    int32_t wmax, ecl_graph* out, int32_t* family) {
   if (!out || nmin < 1 || nmax < nmin || index < 0) return ECL_ERR_INVALID_ARG;
-  const uint64_t seed = seed0 + (uint64_t)index;
-  const uint64_t r0 = ecl_rng(seed, 5, 0), r1 = ecl_rng(seed, 5, 1);
-  const int fam = (int)(r0 % 4);
-  const double u = (double)(r1 >> 11) * (1.0 / 9007199254740992.0);
-  const double ln = std::log((double)nmin) + u * (std::log((double)nmax) - std::log((double)nmin));
-  const int32_t n = (int32_t)std::max<double>(nmin, std::min<double>(nmax, std::llround(std::exp(ln))));
-  if (family) *family = fam;
-  switch (fam) {
-    case 0: {
-      const int32_t rows = std::max<int32_t>(1, (int32_t)std::sqrt((double)n));
-      return ecl_gen_grid(rows, std::max<int32_t>(1, n / rows), seed, wmax, 1, out);
-    }
+  const EclBatchPick p = ecl_batch_pick(index, seed0, nmin, nmax);
+  if (family) *family = p.family;
+  switch (p.family) {
+    case 0:
+      return ecl_gen_grid(p.rows_or_scale, std::max<int32_t>(1, p.nodes / p.rows_or_scale), p.seed, wmax, 1,
+                          out);
     case 1:
-      return ecl_gen_er(n, 8.0, seed, wmax, 1, out);
-    case 2: {
-      const int32_t scale = std::max<int32_t>(1, (int32_t)std::lround(std::log2((double)n)));
-      return ecl_gen_rmat(scale, 8, 0.57, 0.19, 0.19, seed, wmax, 1, out);
-    }
+      return ecl_gen_er(p.nodes, kBatchErDegree, p.seed, wmax, 1, out);
+    case 2:
+      return ecl_gen_rmat(p.rows_or_scale, kBatchRmatEdgeFactor, kBatchRmatA, kBatchRmatB, kBatchRmatC, p.seed,
+                          wmax, 1, out);
     default:
-      return ecl_gen_rgg2d(n, 3.0, seed, wmax, 1, out);
+      return ecl_gen_rgg2d(p.nodes, kBatchRggDegree, p.seed, wmax, 1, out);
   }
 }

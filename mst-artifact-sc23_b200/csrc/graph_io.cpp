@@ -117,13 +117,7 @@ extern "C" int ecl_synthesize_weights(ecl_graph* g) {
   if (!g || !g->eweight || !g->nindex || g->nodes < 1) return ECL_ERR_INVALID_ARG;
   for (int32_t i = 0; i < g->nodes; i++) {
     for (int32_t j = g->nindex[i]; j < g->nindex[i + 1]; j++) {
-      const int32_t k = g->nlist[j];
-      // i*k overflows int in the reference for large graphs; it wraps modulo
-      // 2^32 on every compiler the artifact targets, so do exactly that.
-      const int32_t prod = (int32_t)((uint32_t)i * (uint32_t)k);
-      int32_t w = 1 + (prod % g->nodes);
-      if (w < 0) w = -w;
-      g->eweight[j] = w;
+      g->eweight[j] = ecl_synth_weight(i, g->nlist[j], g->nodes);
     }
   }
   return ECL_OK;

@@ -47,3 +47,44 @@ uint32_t ecl_sample_hash(uint32_t val);
 int ecl_heuristic_threshold_arrays(int32_t nodes, int32_t edges,
                                    const int32_t* eweight, int32_t* threshold,
                                    int32_t* filtered);
+
+// The reference's weight for a weightless input (ECL_MST.cu:410-419):
+// 1 + ((i * k) % nodes), made non-negative. i * k wraps modulo 2^32 as int
+// arithmetic does on every compiler the artifact targets.
+ECL_HD int32_t ecl_synth_weight(int32_t i, int32_t k, int32_t nodes) {
+  const int32_t prod = (int32_t)((uint32_t)i * (uint32_t)k);
+  int32_t w = 1 + (prod % nodes);
+  return w < 0 ? -w : w;
+}
+
+// Shared parameters of the synthetic families, so the host generators and the
+// device generators (preprocess.cu) draw exactly the same graphs.
+struct EclRmatCut {
+  uint32_t ta, tab, tabc;  // quadrant thresholds in 16-bit fixed point
+};
+EclRmatCut ecl_rmat_cut(double a, double b, double c);
+
+struct EclRggGrid {
+  uint64_t r2;      // squared radius, 31-bit fixed point units
+  int64_t cells;    // cells per side
+  uint64_t cell_w;  // cell width
+};
+EclRggGrid ecl_rgg_grid(int32_t nodes, double avg_degree);
+
+// Family (0 grid, 1 ER, 2 RMAT, 3 RGG2D), vertex count and seed of graph
+// `index` of the mixed batch. rows_or_scale is the grid's row count or the
+// RMAT scale (unused for the other families).
+struct EclBatchPick {
+  int family;
+  int32_t nodes;
+  int32_t rows_or_scale;
+  uint64_t seed;
+};
+EclBatchPick ecl_batch_pick(int32_t index, uint64_t seed0, int32_t nmin, int32_t nmax);
+
+// Families of the mixed batch (besides the grid): ER with average degree 8,
+// RMAT (0.57, 0.19, 0.19) with edge factor 8, RGG2D with average degree 3.
+constexpr double kBatchErDegree = 8.0;
+constexpr int32_t kBatchRmatEdgeFactor = 8;
+constexpr double kBatchRmatA = 0.57, kBatchRmatB = 0.19, kBatchRmatC = 0.19;
+constexpr double kBatchRggDegree = 3.0;

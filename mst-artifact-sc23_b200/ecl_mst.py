@@ -140,6 +140,22 @@ def load():
         "ecl_mlp_grad": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, POINTER(c_float)]),
         "ecl_mlp_train": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_float, c_void_p]),
         "ecl_verify": (c_int, [G, c_void_p, c_void_p, POINTER(c_int64), POINTER(c_uint64), POINTER(c_uint64)]),
+        "ecl_csr_from_pairs_device": (c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_int32, c_uint64,
+                                              c_int32, c_void_p, G]),
+        "ecl_gen_grid_device": (c_int, [c_int32, c_int32, c_uint64, c_int32, c_void_p, G]),
+        "ecl_gen_er_device": (c_int, [c_int32, c_double, c_uint64, c_int32, c_void_p, G]),
+        "ecl_gen_rmat_device": (c_int, [c_int32, c_int32, c_double, c_double, c_double, c_uint64, c_int32,
+                                        c_void_p, G]),
+        "ecl_gen_rgg2d_device": (c_int, [c_int32, c_double, c_uint64, c_int32, c_void_p, G]),
+        "ecl_gen_batch_graph_device": (c_int, [c_int32, c_uint64, c_int32, c_int32, c_int32, c_void_p, G,
+                                               POINTER(c_int32)]),
+        "ecl_free_device_graph": (None, [G]),
+        "ecl_graph_to_host": (c_int, [G, G]),
+        "ecl_gen_batch_device": (c_int, [c_int32, c_uint64, c_int32, c_int32, c_int32, c_int32, c_void_p,
+                                         POINTER(EclBatchC), c_void_p]),
+        "ecl_free_device_batch": (None, [POINTER(EclBatchC)]),
+        "ecl_write_pbbs": (c_int, [G, c_char_p]),
+        "ecl_write_mtx": (c_int, [G, c_char_p]),
         "ecl_forest_weight": (c_uint64, [G, c_void_p]),
     }
     for name, (res, args) in sig.items():
@@ -251,6 +267,155 @@ def gen_batch(count, seed0=1000, nmin=1000, nmax=2_000_000, wmax=1 << 20, thread
     workers = threads or os.cpu_count() or 1
     with ThreadPoolExecutor(workers) as ex:
         return list(ex.map(lambda i: gen_batch_graph(i, seed0, nmin, nmax, wmax)[0], range(count)))
+
+
+def write_pbbs(g, path):
+    """PBBS WeightedEdgeArray text, as PBBS_CPU/inputs/ecl2pbbs_genweights.cpp writes it."""
+    gs = g.struct()
+    _check(load().ecl_write_pbbs(ctypes.byref(gs), os.fsencode(path)), f"write_pbbs {path}")
+
+
+def write_mtx(g, path):
+    """MatrixMarket text, as cuGraph_GPU/inputs/ecl2mtx_genweights_cugraph.cpp writes it."""
+    gs = g.struct()
+    _check(load().ecl_write_mtx(ctypes.byref(gs), os.fsencode(path)), f"write_mtx {path}")
+
+
+# ------------------------------------------------------ GPU-side preprocessing
+WEIGHTS_GIVEN, WEIGHTS_HASH, WEIGHTS_SYNTH = 0, 1, 2
+
+
+class DeviceGraph:
+    """An ECLgraph whose arrays live in device memory (cudaMalloc'd by the
+    library); ``to_host()`` copies it into a ``Graph``."""
+
+    def __init__(self, gc):
+        self._lib = load()
+        self.c = gc
+        self.nodes, self.edges = gc.nodes, gc.edges
+
+    @property
+    def d_nindex(self):
+        return self.c.nindex
+
+    @property
+    def d_nlist(self):
+        return self.c.nlist
+
+    @property
+    def d_eweight(self):
+        return self.c.eweight
+
+    def to_host(self):
+        h = EclGraphC()
+        _check(self._lib.ecl_graph_to_host(ctypes.byref(self.c), ctypes.byref(h)), "graph_to_host")
+        return Graph._from_c(h)
+
+    def close(self):
+        if self.c.nindex:
+            self._lib.ecl_free_device_graph(ctypes.byref(self.c))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _device_graph(fn, what, *args):
+    gc = EclGraphC()
+    _check(fn(*args, ctypes.byref(gc)), what)
+    return DeviceGraph(gc)
+
+
+def csr_from_pairs_device(nodes, pairs, d_u, d_v, d_w=None, rule=WEIGHTS_HASH, seed=0, wmax=1, stream=None):
+    """Symmetric deduplicated CSR from `pairs` device-resident undirected pairs."""
+    return _device_graph(load().ecl_csr_from_pairs_device, "csr_from_pairs_device", nodes, pairs, d_u, d_v, d_w,
+                         rule, seed, wmax, stream)
+
+
+def gen_grid_device(rows, cols, seed, wmax, stream=None):
+    return _device_graph(load().ecl_gen_grid_device, "gen_grid_device", rows, cols, seed, wmax, stream)
+
+
+def gen_er_device(nodes, avg_degree, seed, wmax, stream=None):
+    return _device_graph(load().ecl_gen_er_device, "gen_er_device", nodes, avg_degree, seed, wmax, stream)
+
+
+def gen_rmat_device(scale, edge_factor, a, b, c, seed, wmax, stream=None):
+    return _device_graph(load().ecl_gen_rmat_device, "gen_rmat_device", scale, edge_factor, a, b, c, seed, wmax,
+                         stream)
+
+
+def gen_rgg2d_device(nodes, avg_degree, seed, wmax, stream=None):
+    return _device_graph(load().ecl_gen_rgg2d_device, "gen_rgg2d_device", nodes, avg_degree, seed, wmax, stream)
+
+
+def gen_batch_graph_device(index, seed0=1000, nmin=1000, nmax=2_000_000, wmax=1 << 20, stream=None):
+    """Graph `index` of the mixed batch drawn on the device: (DeviceGraph, family)."""
+    gc = EclGraphC()
+    fam = c_int32()
+    _check(load().ecl_gen_batch_graph_device(index, seed0, nmin, nmax, wmax, stream, ctypes.byref(gc),
+                                             ctypes.byref(fam)), "gen_batch_graph_device")
+    return DeviceGraph(gc), fam.value
+
+
+class DeviceBatch:
+    """The first `count` graphs of the mixed batch, drawn on the device and
+    packed into one batch layout (ecl_gen_batch_device). Same interface as
+    ``Batch`` for ``BatchContext``; the arrays stay on the device."""
+
+    def __init__(self, count, seed0=1000, nmin=1000, nmax=2_000_000, wmax=1 << 20, align=4, stream=None):
+        self._lib = load()
+        self.c = EclBatchC()
+        fam = np.zeros(count, np.int32)
+        _check(self._lib.ecl_gen_batch_device(count, seed0, nmin, nmax, wmax, align, stream, ctypes.byref(self.c),
+                                              _ptr(fam)), "gen_batch_device")
+        self.family = fam
+        self.num_graphs = count
+
+        def arr(p, ct, dt):
+            return np.ctypeslib.as_array(ctypes.cast(p, POINTER(ct)), (count,)).astype(dt)
+
+        self.nodes = arr(self.c.nodes, c_int32, np.int32)
+        self.edges = arr(self.c.edges, c_int32, np.int32)
+        self.nindex_off = arr(self.c.nindex_off, c_int64, np.int64)
+        self.edge_off = arr(self.c.edge_off, c_int64, np.int64)
+        self.total_nindex = int(self.nindex_off[-1]) + -(-(int(self.nodes[-1]) + 1) // align) * align
+        self.total_edges = int(self.edge_off[-1]) + -(-max(int(self.edges[-1]), 1) // align) * align
+        self.d_nindex, self.d_nlist, self.d_eweight = self.c.nindex, self.c.nlist, self.c.eweight
+
+    def struct(self, d_nindex=None, d_nlist=None, d_eweight=None):
+        return EclBatchC(self.num_graphs, self.c.nodes, self.c.edges, self.c.nindex_off, self.c.edge_off,
+                         d_nindex or self.d_nindex, d_nlist or self.d_nlist, d_eweight or self.d_eweight)
+
+    def slice(self, inmst, g):
+        a = int(self.edge_off[g])
+        return inmst[a:a + int(self.edges[g])]
+
+    def graph(self, g):
+        """Host copy of graph g."""
+        gc = EclGraphC(int(self.nodes[g]), int(self.edges[g]), self.d_nindex + 4 * int(self.nindex_off[g]),
+                       self.d_nlist + 4 * int(self.edge_off[g]), self.d_eweight + 4 * int(self.edge_off[g]))
+        h = EclGraphC()
+        _check(self._lib.ecl_graph_to_host(ctypes.byref(gc), ctypes.byref(h)), "graph_to_host")
+        return Graph._from_c(h)
+
+    def close(self):
+        if self.c.nindex:
+            self._lib.ecl_free_device_batch(ctypes.byref(self.c))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def heuristic_threshold(g):
