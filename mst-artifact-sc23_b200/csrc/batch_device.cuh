@@ -178,7 +178,7 @@ __device__ void cta_rounds(RoundArgs& ra, unsigned* cnt, RoundSmem& s) {
     int4* out = odd ? ra.wl0 : ra.wl1;
     u64* mcur = odd ? ra.minv1 : ra.minv0;
     u64* mprev = odd ? ra.minv0 : ra.minv1;
-    round_find_min(ra, in, W, out, &cnt[r + 1], mcur, mprev, r > 0, 0u, 1u, s);
+    round_find_min(ra, in, W, out, &cnt[r + 1], &cnt[ECL_MAX_ROUNDS + 1], mcur, mprev, r > 0, 0u, 1u, s);
     __syncthreads();
     const unsigned W2 = min(((volatile unsigned*)cnt)[r + 1], ra.wl_cap);
     r++;
@@ -196,7 +196,7 @@ __device__ void cta_rounds(RoundArgs& ra, unsigned* cnt, RoundSmem& s) {
 
 __global__ void __launch_bounds__(kThreads, 2) k_batch_small(BatchArgs b) {
   __shared__ RoundSmem s;
-  __shared__ unsigned cnt[ECL_MAX_ROUNDS + 1];
+  __shared__ unsigned cnt[ECL_MAX_ROUNDS + 2];  // per-round entry counts, then a kept-count sink
   __shared__ int sh_g, sh_thr, sh_filtered;
   int* parent = b.parent_pool + (size_t)blockIdx.x * b.cap_n;
   u64* minv0 = b.minv_pool + (size_t)blockIdx.x * 2 * b.cap_n;
@@ -247,6 +247,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_small(BatchArgs b) {
     ra.small_tail = 0;
     ra.count_atomics = b.count_atomics;
     ra.abl = b.abl;
+    ra.chunk = 0;  // one CTA per graph: the per-tile reservation costs no grid-wide waits
     cta_scan<kLight>(ni, nl, ew, n, m, thr, parent, wl0, ra.wl_cap, &cnt[0], out, b.st, s.rs);
     __syncthreads();
     cta_rounds(ra, cnt, s);

@@ -117,6 +117,10 @@ struct RoundArgs {
   unsigned small_tail;
   int count_atomics;
   unsigned abl;  // kAbl* bits: techniques switched off to measure what they buy
+  // Worklist slots a warp of the find/min pass reserves at once (0: one
+  // reservation per CTA tile, with two CTA barriers per tile). The host sizes
+  // it so that every warp's unused chunk tail fits in the worklist's slack.
+  unsigned chunk;
 };
 
 // Ablation switches of the round kernel (mst_opts flags ECL_FLAG_NO_*).
@@ -328,6 +332,7 @@ constexpr int kScanWarps = 8;                        // consumer warps of a scan
 constexpr int kScanThreads = (kScanWarps + 1) * 32;  // plus the producer warp
 constexpr int kScanSegCap = 2048;                    // longest nindex slice (vertices) staged per tile
 constexpr unsigned kScanMaxChunk = 64;               // worklist slots a warp reserves at once
+constexpr unsigned kRoundMaxChunk = 256;             // the same for a warp of the round kernel
 
 // ring stages and the resident CTAs per SM the launch bounds ask for, per EPT
 #ifndef ECL_SCAN_S4
@@ -710,6 +715,7 @@ __global__ void __launch_bounds__(kThreads) k_flatten(int* parent, int n, const 
 // L2 address; these small direct-mapped tables absorb the repeats per CTA.
 struct RoundSmem {
   ReserveSmem rs;
+  unsigned kept;             // entries the CTA kept in the current find/min pass
   int hot_rep[kHotSlots];    // hot representative -> CTA-local partial minimum
   u64 hot_key[kHotSlots];
   int reset_seen[kHotSlots]; // previous-round slots this CTA already cleared
@@ -722,6 +728,7 @@ __device__ __forceinline__ unsigned hot_slot(int r) { return ((unsigned)r * 0x9E
 __device__ __forceinline__ unsigned find_slot(int r) { return ((unsigned)r * 0x85EBCA6Bu) >> (32 - kFindLog); }
 
 __device__ __forceinline__ void round_smem_clear(RoundSmem& s) {
+  if (threadIdx.x == 0) s.kept = 0;
   for (int i = threadIdx.x; i < kHotSlots; i += blockDim.x) {
     s.hot_rep[i] = -1;
     s.hot_key[i] = kNoEdge;
@@ -975,13 +982,23 @@ __device__ __forceinline__ void offer_mins(const int (&rep)[N], const u64 (&key)
 // `out` with the reps (implicit path compression, :218-219) and offers its
 // key to both reps' min slots.
 __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* in, unsigned W,
-                                               int4* out, unsigned* out_ctr, u64* mcur, u64* mprev,
-                                               bool reset, unsigned start, unsigned stride,
-                                               RoundSmem& s) {
+                                               int4* out, unsigned* out_ctr, unsigned* kept_ctr,
+                                               u64* mcur, u64* mprev, bool reset, unsigned start,
+                                               unsigned stride, RoundSmem& s) {
   constexpr int N = 2 * kEPT;
   const unsigned tile = blockDim.x * kEPT;
   const unsigned ntiles = (W + tile - 1) / tile;
   unsigned long long atomics = 0;
+  const bool dedup = (a.abl & kDedup) != 0;
+  const bool chunked = a.chunk != 0 && !dedup;  // uniform across the grid
+  const int lane = threadIdx.x & 31;
+  unsigned wpos = 0, wend = 0;  // chunked: this warp's reserved, unused slots [wpos, wend)
+  unsigned kept = 0;            // entries this thread kept
+  // Chunk size for this pass: about a quarter of a warp's expected share of
+  // the input, between 32 and the host's bound, so that the unused tails
+  // (at most chunk - 1 null entries per warp) stay small against W.
+  const unsigned warps = (stride * blockDim.x) >> 5;
+  const unsigned wchunk = chunked ? max(32u, min(a.chunk, W / (4u * warps))) : 0u;
   for (unsigned t = start; t < ntiles; t += stride) {
     int4 e[kEPT];
     bool in_range[kEPT];
@@ -990,7 +1007,7 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
       const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
       in_range[k] = idx < W;
       e[k] = in_range[k] ? __ldcg(in + idx) : make_int4(0, 0, 0, 0);
-      if (e[k].x < 0) in_range[k] = false;  // null entry (unused scan slot)
+      if (e[k].x < 0) in_range[k] = false;  // null entry (unused chunk tail)
     }
     int v[N];
     bool vv[N];
@@ -1012,23 +1029,63 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
       e[k].x = v[2 * k];
       e[k].y = v[2 * k + 1];
     }
-    unsigned pos;
-    drop_parallel_reserve<kEPT>(e, keep, out_ctr, s, &pos, (a.abl & kDedup) != 0);
+    // Output slots: a warp takes them from its own chunk and reserves a fresh
+    // one with a single atomic when the chunk runs out, so warps never wait
+    // for each other; without chunks the CTA reserves once per tile.
+    // Rank q of the warp's survivors goes to cur + q while q < avail (the old
+    // chunk), then to fresh + (q - avail). Without chunks, cur is this
+    // thread's first slot and avail is unbounded.
+    unsigned q = 0, cur = 0, avail = ~0u, fresh = 0;
+    if (chunked) {
+      unsigned cnt = 0;
+#pragma unroll
+      for (int k = 0; k < kEPT; k++) cnt += keep[k];
+      unsigned incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
+      }
+      const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+      q = incl - cnt;
+      cur = wpos;
+      avail = wend - wpos;
+      if (total > avail) {
+        const unsigned take = max(total - avail, wchunk);
+        if (lane == 0) fresh = atomicAdd(out_ctr, take);
+        fresh = __shfl_sync(0xffffffffu, fresh, 0);
+        wpos = fresh + (total - avail);
+        wend = fresh + take;
+      } else {
+        wpos += total;
+      }
+    } else {
+      drop_parallel_reserve<kEPT>(e, keep, out_ctr, s, &cur, dedup);
+    }
     u64 key[N];
     bool kv[N];
 #pragma unroll
     for (int k = 0; k < kEPT; k++) {
       if (keep[k]) {
+        const unsigned pos = q < avail ? cur + q : fresh + (q - avail);
         if (pos < a.wl_cap) out[pos] = e[k];
         else atomicOr(&a.st->error, kErrOverflow);
-        pos++;
+        q++;
+        kept++;
       }
       key[2 * k] = key[2 * k + 1] = edge_key(e[k].z, e[k].w);
       kv[2 * k] = kv[2 * k + 1] = keep[k];
     }
     offer_mins<N>(v, key, kv, mcur, s, atomics, !(a.abl & kAblNoCoop), !(a.abl & kAblNoGuards));
   }
+  if (chunked)  // null entries in the warp's unused chunk tail
+    for (unsigned p = wpos + lane; p < wend; p += 32)
+      if (p < a.wl_cap) out[p] = make_int4(-1, -1, 0, 0);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+  if (lane == 0 && kept) atomicAdd(&s.kept, kept);
   __syncthreads();
+  if (threadIdx.x == 0 && s.kept) atomicAdd(kept_ctr, s.kept);
   // flush the CTA's partial minima of hot representatives
   for (int i = threadIdx.x; i < kHotSlots; i += blockDim.x) {
     const int r = s.hot_rep[i];
@@ -1067,6 +1124,7 @@ __device__ __forceinline__ void round_mark(const RoundArgs& a, const int4* wl, u
       const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
       in_range[k] = idx < W;
       e[k] = in_range[k] ? __ldcg(wl + idx) : make_int4(0, 0, 0, 0);
+      if (e[k].x < 0) in_range[k] = false;  // null entry (unused chunk tail)
     }
     u64 mx[kEPT], my[kEPT];
 #pragma unroll
@@ -1119,7 +1177,8 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
     int4* out = odd ? a.wl0 : a.wl1;
     u64* mcur = odd ? a.minv1 : a.minv0;
     u64* mprev = odd ? a.minv0 : a.minv1;
-    round_find_min(a, in, W, out, &st->wl_count[ph][r + 1], mcur, mprev, r > 0, start, stride, s);
+    round_find_min(a, in, W, out, &st->wl_count[ph][r + 1], &st->wl_kept[ph][r + 1], mcur, mprev, r > 0,
+                   start, stride, s);
     if (tail) __syncthreads();
     else if (!grid_barrier(st, kBarrierTimeoutNs)) return;
     if (stamp) st->t_round[ph][2 * r] = globaltimer_ns();

@@ -44,6 +44,7 @@ struct DevState {
   u64 t_round_start[2];
   u64 t_round[2][2 * ECL_MAX_ROUNDS];
   unsigned scan_kept[2];  // entries each scan kept (wl_count[p][0] also counts padding)
+  unsigned wl_kept[2][ECL_MAX_ROUNDS + 1];  // [phase][r + 1] = entries round r kept (no padding)
 };
 
 __device__ __forceinline__ u64 globaltimer_ns() {

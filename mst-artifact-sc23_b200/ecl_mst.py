@@ -33,6 +33,8 @@ FLAG_L2_PERSIST, FLAG_STATS, FLAG_NO_SMALL_TAIL = 1, 2, 4
 FLAG_NO_GUARDS, FLAG_NO_WARP_COOP, FLAG_DEDUP, FLAG_NO_FIND_CACHE = 8, 16, 32, 64
 # direct launches instead of replaying a captured solve (keeps per-phase timings)
 FLAG_NO_GRAPH = 128
+# round worklist slots reserved per CTA tile instead of per-warp chunks (ablation)
+FLAG_CTA_RESERVE = 256
 MAX_ROUNDS = 64
 
 
@@ -60,7 +62,8 @@ class MstStats(ctypes.Structure):
                 ("wl_in", (c_int64 * MAX_ROUNDS) * 2), ("atomics", c_int64),
                 ("forest_edges", c_int64), ("forest_weight", c_uint64),
                 ("ms_total", c_float), ("ms_rounds", c_float), ("ms_scan", c_float),
-                ("us_scan", (c_float * 3) * 2), ("us_round", ((c_float * 2) * MAX_ROUNDS) * 2)]
+                ("us_scan", (c_float * 3) * 2), ("us_round", ((c_float * 2) * MAX_ROUNDS) * 2),
+                ("wl_real", (c_int64 * MAX_ROUNDS) * 2)]
 
     def as_dict(self):
         return {
@@ -68,6 +71,7 @@ class MstStats(ctypes.Structure):
             "degree_split": self.degree_split, "rounds": list(self.rounds),
             "status": self.status, "scan_kept": list(self.scan_kept),
             "wl_in": [[int(x) for x in self.wl_in[p][: max(self.rounds[p], 0) + 1]] for p in range(2)],
+            "wl_real": [[int(x) for x in self.wl_real[p][: max(self.rounds[p], 0) + 1]] for p in range(2)],
             "atomics": self.atomics, "forest_edges": self.forest_edges,
             "forest_weight": self.forest_weight, "ms_total": self.ms_total,
             "ms_rounds": self.ms_rounds, "ms_scan": self.ms_scan,

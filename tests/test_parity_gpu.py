@@ -26,6 +26,7 @@ MODES = [
     dict(flags=E.FLAG_NO_WARP_COOP),
     dict(flags=E.FLAG_DEDUP),
     dict(flags=E.FLAG_NO_FIND_CACHE),
+    dict(flags=E.FLAG_CTA_RESERVE),
     dict(flags=E.FLAG_NO_GUARDS | E.FLAG_NO_WARP_COOP | E.FLAG_DEDUP | E.FLAG_NO_FIND_CACHE
          | E.FLAG_NO_SMALL_TAIL, mode=E.THRESH_NONE),
 ]
@@ -193,6 +194,14 @@ def test_stats_are_consistent(ctx):
     assert st["scan_kept"][0] == light
     assert light <= st["wl_in"][0][0] <= light + 148 * 4 * 8 * 63
     assert 0 < st["scan_kept"][1] <= st["wl_in"][1][0]
+    # rounds: the real entries never grow and stay within the slots (which add chunk-tail nulls)
+    for p in range(2):
+        real, slots = st["wl_real"][p], st["wl_in"][p]
+        assert real[0] == st["scan_kept"][p]
+        for r in range(st["rounds"][p]):
+            assert real[r] <= slots[r]
+            if r + 1 <= st["rounds"][p] and r + 1 < len(real):
+                assert real[r + 1] <= real[r]
     assert st["atomics"] > 0
     assert st["ms_total"] > 0
     assert st["forest_edges"] <= g.nodes - 1
