@@ -152,7 +152,7 @@ def round_kernel_bytes(st, entry_bytes=16, atomics=None):
     A = guarded atomics actually issued when counted, else 2*W_out (upper bound).
     """
     total = 0
-    wl = st.get("wl_real") or st["wl_in"]  # real entries: chunk-tail nulls are not algorithmic
+    wl = st.get("wl_real") or st["wl_in"]  # real entries: the scans' null padding is not algorithmic
     for p in range(2):
         w = wl[p]
         for r in range(st["rounds"][p]):
@@ -481,8 +481,7 @@ def main():
                   ("NAG_NW_NF", E_.FLAG_NO_GUARDS | E_.FLAG_NO_WARP_COOP, E_.THRESH_NONE),
                   ("with_dedup", E_.FLAG_DEDUP, E_.THRESH_HEURISTIC),
                   ("no_find_cache", E_.FLAG_NO_FIND_CACHE, E_.THRESH_HEURISTIC),
-                  ("no_small_tail", E_.FLAG_NO_SMALL_TAIL, E_.THRESH_HEURISTIC),
-                  ("cta_reserve", E_.FLAG_CTA_RESERVE, E_.THRESH_HEURISTIC)]
+                  ("no_small_tail", E_.FLAG_NO_SMALL_TAIL, E_.THRESH_HEURISTIC)]
         ablation, base_ms, ref_hash = {}, None, None
         for name, flags, tmode in series:
             o = E_.make_opts(mode=tmode, degree_split=args.split, flags=flags)

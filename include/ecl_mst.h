@@ -205,10 +205,7 @@ enum {
    * the first repeat and replayed as one launch after that; a replayed
    * solve's stats carry ms_total only. NO_GRAPH keeps direct launches (and
    * the per-phase timings). */
-  ECL_FLAG_NO_GRAPH = 1 << 7,
-  /* Round worklist slots reserved once per CTA tile (two CTA barriers per
-   * tile) instead of in per-warp chunks (ablation). */
-  ECL_FLAG_CTA_RESERVE = 1 << 8
+  ECL_FLAG_NO_GRAPH = 1 << 7
 };
 
 typedef struct mst_opts {
@@ -262,7 +259,7 @@ typedef struct ecl_mst_stats {
                               scan, flatten, heavy scan kernel}                */
   float us_round[2][ECL_MAX_ROUNDS][2]; /* per round: find/min pass, mark pass  */
   int64_t wl_real[2][ECL_MAX_ROUNDS];   /* entries entering each round without
-                                           the null padding of chunk tails    */
+                                           the scans' null padding            */
 } ecl_mst_stats;
 
 /* ------------------------------------------------------------- the solve */

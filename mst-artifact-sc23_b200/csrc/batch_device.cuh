@@ -247,7 +247,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_small(BatchArgs b) {
     ra.small_tail = 0;
     ra.count_atomics = b.count_atomics;
     ra.abl = b.abl;
-    ra.chunk = 0;  // one CTA per graph: the per-tile reservation costs no grid-wide waits
     cta_scan<kLight>(ni, nl, ew, n, m, thr, parent, wl0, ra.wl_cap, &cnt[0], out, b.st, s.rs);
     __syncthreads();
     cta_rounds(ra, cnt, s);

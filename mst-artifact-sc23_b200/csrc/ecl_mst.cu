@@ -21,7 +21,7 @@ using namespace ecl;
 namespace {
 constexpr int kDefaultSplit = 8;
 constexpr unsigned kDefaultSmallTail = 4096;
-constexpr int64_t kWlSlack = 1 << 21;  // worklist slots beyond `edges` (scan / round chunk tails)
+constexpr int64_t kWlSlack = 1 << 19;  // worklist slots beyond `edges` (scan chunk tails)
 constexpr int kLearnedMinEdges = 1 << 20;
 }  // namespace
 
@@ -119,16 +119,6 @@ int enqueue_prep(const PrepArgs& pa, int sm_count, cudaStream_t s) {
 }
 
 // Round-kernel ablation bits from the option flags.
-// Worklist slots a round warp reserves at once: the unused tails (at most
-// chunk - 1 per warp) must fit in `slack`; below 32 slots per warp the
-// per-tile CTA reservation is used instead (chunk 0).
-unsigned round_chunk(int flags, int64_t slack, int grid) {
-  if (flags & ECL_FLAG_CTA_RESERVE) return 0;
-  const int64_t warps = (int64_t)grid * (kRoundThreads / 32);
-  const int64_t c = std::min<int64_t>(kRoundMaxChunk, slack / std::max<int64_t>(warps, 1));
-  return c >= 32 ? (unsigned)c : 0u;
-}
-
 unsigned round_ablation(int flags) {
   return ((flags & ECL_FLAG_NO_GUARDS) ? kAblNoGuards : 0u) | ((flags & ECL_FLAG_NO_WARP_COOP) ? kAblNoCoop : 0u) |
          ((flags & ECL_FLAG_DEDUP) ? kDedup : 0u) | ((flags & ECL_FLAG_NO_FIND_CACHE) ? kAblNoFindCache : 0u);
@@ -354,7 +344,6 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   ra.count_atomics = (o->flags & ECL_FLAG_STATS) ? 1 : 0;
   ra.abl = round_ablation(o->flags);
   const int rgrid = std::max(1, std::min(c->round_grid, (m / 2 + kRoundThreads - 1) / kRoundThreads + 1));
-  ra.chunk = round_chunk(o->flags, (int64_t)sa.wl_slack, rgrid);  // a round keeps at most m entries too
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[5], s));
   if ((st = launch_scans<kLight>(device_split, split, sa, s))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[1], s));
@@ -771,7 +760,6 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   ra.count_atomics = (o.flags & ECL_FLAG_STATS) ? 1 : 0;
   ra.abl = round_ablation(o.flags);
   const int rgrid = std::max(1, std::min(d->round_grid, (m / 2 + kRoundThreads - 1) / kRoundThreads + 1));
-  ra.chunk = round_chunk(o.flags, (int64_t)sa.wl_slack, rgrid);
   if ((st = launch_scan<kLight>(scan_ept(split), sa, s))) return st;
   ra.phase = 0;
   if ((st = launch_coop((const void*)k_rounds, rgrid, kRoundThreads, &ra, s))) return st;

@@ -117,10 +117,6 @@ struct RoundArgs {
   unsigned small_tail;
   int count_atomics;
   unsigned abl;  // kAbl* bits: techniques switched off to measure what they buy
-  // Worklist slots a warp of the find/min pass reserves at once (0: one
-  // reservation per CTA tile, with two CTA barriers per tile). The host sizes
-  // it so that every warp's unused chunk tail fits in the worklist's slack.
-  unsigned chunk;
 };
 
 // Ablation switches of the round kernel (mst_opts flags ECL_FLAG_NO_*).
@@ -332,7 +328,6 @@ constexpr int kScanWarps = 8;                        // consumer warps of a scan
 constexpr int kScanThreads = (kScanWarps + 1) * 32;  // plus the producer warp
 constexpr int kScanSegCap = 2048;                    // longest nindex slice (vertices) staged per tile
 constexpr unsigned kScanMaxChunk = 64;               // worklist slots a warp reserves at once
-constexpr unsigned kRoundMaxChunk = 256;             // the same for a warp of the round kernel
 
 // ring stages and the resident CTAs per SM the launch bounds ask for, per EPT
 #ifndef ECL_SCAN_S4
@@ -715,7 +710,7 @@ __global__ void __launch_bounds__(kThreads) k_flatten(int* parent, int n, const 
 // L2 address; these small direct-mapped tables absorb the repeats per CTA.
 struct RoundSmem {
   ReserveSmem rs;
-  unsigned kept;             // entries the CTA kept in the current find/min pass
+  unsigned kept;             // entries the CTA kept in the current find/min pass (tile totals)
   int hot_rep[kHotSlots];    // hot representative -> CTA-local partial minimum
   u64 hot_key[kHotSlots];
   int reset_seen[kHotSlots]; // previous-round slots this CTA already cleared
@@ -823,7 +818,10 @@ __device__ __forceinline__ void drop_parallel_reserve(const int4 (&e)[E], bool (
       if (lane >= o) x0 += t;
     }
     if (lane < nw) s.rs.warp_off[lane][0] = x0 - w0;
-    if (lane == 31) s.rs.base[0] = x0 ? atomicAdd(ctr, x0) : 0u;
+    if (lane == 31) {
+      s.rs.base[0] = x0 ? atomicAdd(ctr, x0) : 0u;
+      s.kept += x0;  // the tile's survivors (one thread updates it)
+    }
   }
   __syncthreads();  // S3: offsets and the tile's base are published
   *pos = s.rs.base[0] + s.rs.warp_off[warp][0] + (incl - cnt);
@@ -989,16 +987,6 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
   const unsigned tile = blockDim.x * kEPT;
   const unsigned ntiles = (W + tile - 1) / tile;
   unsigned long long atomics = 0;
-  const bool dedup = (a.abl & kDedup) != 0;
-  const bool chunked = a.chunk != 0 && !dedup;  // uniform across the grid
-  const int lane = threadIdx.x & 31;
-  unsigned wpos = 0, wend = 0;  // chunked: this warp's reserved, unused slots [wpos, wend)
-  unsigned kept = 0;            // entries this thread kept
-  // Chunk size for this pass: about a quarter of a warp's expected share of
-  // the input, between 32 and the host's bound, so that the unused tails
-  // (at most chunk - 1 null entries per warp) stay small against W.
-  const unsigned warps = (stride * blockDim.x) >> 5;
-  const unsigned wchunk = chunked ? max(32u, min(a.chunk, W / (4u * warps))) : 0u;
   for (unsigned t = start; t < ntiles; t += stride) {
     int4 e[kEPT];
     bool in_range[kEPT];
@@ -1007,7 +995,7 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
       const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
       in_range[k] = idx < W;
       e[k] = in_range[k] ? __ldcg(in + idx) : make_int4(0, 0, 0, 0);
-      if (e[k].x < 0) in_range[k] = false;  // null entry (unused chunk tail)
+      if (e[k].x < 0) in_range[k] = false;  // null entry (unused scan slot)
     }
     int v[N];
     bool vv[N];
@@ -1029,61 +1017,22 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
       e[k].x = v[2 * k];
       e[k].y = v[2 * k + 1];
     }
-    // Output slots: a warp takes them from its own chunk and reserves a fresh
-    // one with a single atomic when the chunk runs out, so warps never wait
-    // for each other; without chunks the CTA reserves once per tile.
-    // Rank q of the warp's survivors goes to cur + q while q < avail (the old
-    // chunk), then to fresh + (q - avail). Without chunks, cur is this
-    // thread's first slot and avail is unbounded.
-    unsigned q = 0, cur = 0, avail = ~0u, fresh = 0;
-    if (chunked) {
-      unsigned cnt = 0;
-#pragma unroll
-      for (int k = 0; k < kEPT; k++) cnt += keep[k];
-      unsigned incl = cnt;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned x = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += x;
-      }
-      const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
-      q = incl - cnt;
-      cur = wpos;
-      avail = wend - wpos;
-      if (total > avail) {
-        const unsigned take = max(total - avail, wchunk);
-        if (lane == 0) fresh = atomicAdd(out_ctr, take);
-        fresh = __shfl_sync(0xffffffffu, fresh, 0);
-        wpos = fresh + (total - avail);
-        wend = fresh + take;
-      } else {
-        wpos += total;
-      }
-    } else {
-      drop_parallel_reserve<kEPT>(e, keep, out_ctr, s, &cur, dedup);
-    }
+    unsigned pos;
+    drop_parallel_reserve<kEPT>(e, keep, out_ctr, s, &pos, (a.abl & kDedup) != 0);
     u64 key[N];
     bool kv[N];
 #pragma unroll
     for (int k = 0; k < kEPT; k++) {
       if (keep[k]) {
-        const unsigned pos = q < avail ? cur + q : fresh + (q - avail);
         if (pos < a.wl_cap) out[pos] = e[k];
         else atomicOr(&a.st->error, kErrOverflow);
-        q++;
-        kept++;
+        pos++;
       }
       key[2 * k] = key[2 * k + 1] = edge_key(e[k].z, e[k].w);
       kv[2 * k] = kv[2 * k + 1] = keep[k];
     }
     offer_mins<N>(v, key, kv, mcur, s, atomics, !(a.abl & kAblNoCoop), !(a.abl & kAblNoGuards));
   }
-  if (chunked)  // null entries in the warp's unused chunk tail
-    for (unsigned p = wpos + lane; p < wend; p += 32)
-      if (p < a.wl_cap) out[p] = make_int4(-1, -1, 0, 0);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
-  if (lane == 0 && kept) atomicAdd(&s.kept, kept);
   __syncthreads();
   if (threadIdx.x == 0 && s.kept) atomicAdd(kept_ctr, s.kept);
   // flush the CTA's partial minima of hot representatives
@@ -1124,7 +1073,6 @@ __device__ __forceinline__ void round_mark(const RoundArgs& a, const int4* wl, u
       const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
       in_range[k] = idx < W;
       e[k] = in_range[k] ? __ldcg(wl + idx) : make_int4(0, 0, 0, 0);
-      if (e[k].x < 0) in_range[k] = false;  // null entry (unused chunk tail)
     }
     u64 mx[kEPT], my[kEPT];
 #pragma unroll

@@ -33,8 +33,6 @@ FLAG_L2_PERSIST, FLAG_STATS, FLAG_NO_SMALL_TAIL = 1, 2, 4
 FLAG_NO_GUARDS, FLAG_NO_WARP_COOP, FLAG_DEDUP, FLAG_NO_FIND_CACHE = 8, 16, 32, 64
 # direct launches instead of replaying a captured solve (keeps per-phase timings)
 FLAG_NO_GRAPH = 128
-# round worklist slots reserved per CTA tile instead of per-warp chunks (ablation)
-FLAG_CTA_RESERVE = 256
 MAX_ROUNDS = 64
 
 
