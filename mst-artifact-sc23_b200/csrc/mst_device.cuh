@@ -979,10 +979,16 @@ __device__ __forceinline__ void offer_mins(const int (&rep)[N], const u64 (&key)
 // array, resolves its endpoints to reps, and if they differ is compacted into
 // `out` with the reps (implicit path compression, :218-219) and offers its
 // key to both reps' min slots.
+//
+// `fresh` marks the first round of a phase: its entries come straight from
+// the scan, so both endpoints are roots (parent[v] = v before the light
+// phase, the flattened light-tree roots before the heavy one) and differ.
+// That round needs no find and keeps every entry: it only offers keys, and
+// the scan's list serves as its output unchanged (no copy).
 __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* in, unsigned W,
                                                int4* out, unsigned* out_ctr, unsigned* kept_ctr,
-                                               u64* mcur, u64* mprev, bool reset, unsigned start,
-                                               unsigned stride, RoundSmem& s) {
+                                               u64* mcur, u64* mprev, bool reset, bool fresh,
+                                               unsigned start, unsigned stride, RoundSmem& s) {
   constexpr int N = 2 * kEPT;
   const unsigned tile = blockDim.x * kEPT;
   const unsigned ntiles = (W + tile - 1) / tile;
@@ -1009,25 +1015,33 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
         reset_prev(e[k].y, mprev, s);
       }
     }
-    multi_find<N>(v, vv, a.parent, s, !(a.abl & kAblNoFindCache));
     bool keep[kEPT];
+    if (fresh) {
 #pragma unroll
-    for (int k = 0; k < kEPT; k++) {
-      keep[k] = in_range[k] && v[2 * k] != v[2 * k + 1];
-      e[k].x = v[2 * k];
-      e[k].y = v[2 * k + 1];
+      for (int k = 0; k < kEPT; k++) keep[k] = in_range[k];
+    } else {
+      multi_find<N>(v, vv, a.parent, s, !(a.abl & kAblNoFindCache));
+#pragma unroll
+      for (int k = 0; k < kEPT; k++) {
+        keep[k] = in_range[k] && v[2 * k] != v[2 * k + 1];
+        e[k].x = v[2 * k];
+        e[k].y = v[2 * k + 1];
+      }
+      unsigned pos;
+      drop_parallel_reserve<kEPT>(e, keep, out_ctr, s, &pos, (a.abl & kDedup) != 0);
+#pragma unroll
+      for (int k = 0; k < kEPT; k++) {
+        if (keep[k]) {
+          if (pos < a.wl_cap) out[pos] = e[k];
+          else atomicOr(&a.st->error, kErrOverflow);
+          pos++;
+        }
+      }
     }
-    unsigned pos;
-    drop_parallel_reserve<kEPT>(e, keep, out_ctr, s, &pos, (a.abl & kDedup) != 0);
     u64 key[N];
     bool kv[N];
 #pragma unroll
     for (int k = 0; k < kEPT; k++) {
-      if (keep[k]) {
-        if (pos < a.wl_cap) out[pos] = e[k];
-        else atomicOr(&a.st->error, kErrOverflow);
-        pos++;
-      }
       key[2 * k] = key[2 * k + 1] = edge_key(e[k].z, e[k].w);
       kv[2 * k] = kv[2 * k + 1] = keep[k];
     }
@@ -1073,6 +1087,7 @@ __device__ __forceinline__ void round_mark(const RoundArgs& a, const int4* wl, u
       const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
       in_range[k] = idx < W;
       e[k] = in_range[k] ? __ldcg(wl + idx) : make_int4(0, 0, 0, 0);
+      if (e[k].x < 0) in_range[k] = false;  // null entry (unused scan slot)
     }
     u64 mx[kEPT], my[kEPT];
 #pragma unroll
@@ -1120,13 +1135,21 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
       if (blockIdx.x != 0) return;
     }
     const unsigned start = tail ? 0u : blockIdx.x, stride = tail ? 1u : gridDim.x;
+    // Round 0 reads the scan's list (wl0) and keeps it as its output; from
+    // round 1 on the lists alternate. The min-slot arrays alternate per round.
+    const bool fresh = r == 0;
+    const bool in1 = !fresh && ((r - 1) & 1) != 0;
+    const int4* in = in1 ? a.wl1 : a.wl0;
+    int4* out = in1 ? a.wl0 : a.wl1;
     const bool odd = (r & 1) != 0;
-    const int4* in = odd ? a.wl1 : a.wl0;
-    int4* out = odd ? a.wl0 : a.wl1;
     u64* mcur = odd ? a.minv1 : a.minv0;
     u64* mprev = odd ? a.minv0 : a.minv1;
     round_find_min(a, in, W, out, &st->wl_count[ph][r + 1], &st->wl_kept[ph][r + 1], mcur, mprev, r > 0,
-                   start, stride, s);
+                   fresh, start, stride, s);
+    if (fresh && blockIdx.x == 0 && threadIdx.x == 0) {  // the scan's list is round 0's output
+      st->wl_count[ph][1] = W;
+      st->wl_kept[ph][1] = st->scan_kept[ph];
+    }
     if (tail) __syncthreads();
     else if (!grid_barrier(st, kBarrierTimeoutNs)) return;
     if (stamp) st->t_round[ph][2 * r] = globaltimer_ns();
@@ -1134,7 +1157,7 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
     r++;
     if (W2 == 0) break;
     hot_refresh(mcur, s);
-    round_mark(a, out, W2, mcur, start, stride, s);
+    round_mark(a, fresh ? in : out, W2, mcur, start, stride, s);
     __syncthreads();
     round_smem_clear(s);
     if (tail) __syncthreads();
