@@ -178,8 +178,8 @@ __device__ void cta_rounds(RoundArgs& ra, unsigned* cnt, RoundSmem& s) {
     int4* out = odd ? ra.wl0 : ra.wl1;
     u64* mcur = odd ? ra.minv1 : ra.minv0;
     u64* mprev = odd ? ra.minv0 : ra.minv1;
-    round_find_min(ra, in, W, out, &cnt[r + 1], &cnt[ECL_MAX_ROUNDS + 1], mcur, mprev, r > 0, false, 0u, 1u,
-                   s);
+    round_find_min(ra, in, W, out, &cnt[r + 1], &cnt[ECL_MAX_ROUNDS + 1], mcur, mprev,
+                   r > 0 ? kResetSparse : kResetNone, false, 0u, 1u, s);
     __syncthreads();
     const unsigned W2 = min(((volatile unsigned*)cnt)[r + 1], ra.wl_cap);
     r++;

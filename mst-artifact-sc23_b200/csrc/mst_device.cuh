@@ -900,6 +900,12 @@ __device__ __forceinline__ void multi_find(int (&v)[N], const bool (&valid)[N], 
     }
 }
 
+// How a find/min pass clears the previous round's min slots: not at all
+// (first round), slot by slot for its entries' reps (deduplicated per CTA),
+// or the whole array with coalesced stores when the entries outnumber the
+// vertices enough that the scattered stores would cost more.
+enum : int { kResetNone = 0, kResetSparse = 1, kResetDense = 2 };
+
 // Clear a previous-round min slot once per CTA.
 __device__ __forceinline__ void reset_prev(int r, u64* mprev, RoundSmem& s) {
   const unsigned slot = hot_slot(r);
@@ -987,12 +993,15 @@ __device__ __forceinline__ void offer_mins(const int (&rep)[N], const u64 (&key)
 // the scan's list serves as its output unchanged (no copy).
 __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* in, unsigned W,
                                                int4* out, unsigned* out_ctr, unsigned* kept_ctr,
-                                               u64* mcur, u64* mprev, bool reset, bool fresh,
+                                               u64* mcur, u64* mprev, int reset, bool fresh,
                                                unsigned start, unsigned stride, RoundSmem& s) {
   constexpr int N = 2 * kEPT;
   const unsigned tile = blockDim.x * kEPT;
   const unsigned ntiles = (W + tile - 1) / tile;
   unsigned long long atomics = 0;
+  if (reset == kResetDense)  // every slot of the previous round's array, coalesced
+    for (unsigned i = start * blockDim.x + threadIdx.x; i < (unsigned)a.nodes; i += stride * blockDim.x)
+      __stcg(mprev + i, kNoEdge);
   for (unsigned t = start; t < ntiles; t += stride) {
     int4 e[kEPT];
     bool in_range[kEPT];
@@ -1010,7 +1019,7 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
       v[2 * k] = e[k].x;
       v[2 * k + 1] = e[k].y;
       vv[2 * k] = vv[2 * k + 1] = in_range[k];
-      if (reset && in_range[k]) {
+      if (reset == kResetSparse && in_range[k]) {
         reset_prev(e[k].x, mprev, s);
         reset_prev(e[k].y, mprev, s);
       }
@@ -1144,7 +1153,9 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
     const bool odd = (r & 1) != 0;
     u64* mcur = odd ? a.minv1 : a.minv0;
     u64* mprev = odd ? a.minv0 : a.minv1;
-    round_find_min(a, in, W, out, &st->wl_count[ph][r + 1], &st->wl_kept[ph][r + 1], mcur, mprev, r > 0,
+    const int reset = fresh ? kResetNone
+                            : (!tail && 4ull * W >= (unsigned long long)a.nodes ? kResetDense : kResetSparse);
+    round_find_min(a, in, W, out, &st->wl_count[ph][r + 1], &st->wl_kept[ph][r + 1], mcur, mprev, reset,
                    fresh, start, stride, s);
     if (fresh && blockIdx.x == 0 && threadIdx.x == 0) {  // the scan's list is round 0's output
       st->wl_count[ph][1] = W;
