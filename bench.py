@@ -141,14 +141,17 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def round_kernel_bytes(st, entry_bytes=16, atomics=None):
+def round_kernel_bytes(st, nodes, entry_bytes=16, atomics=None):
     """Algorithmic bytes of the round kernels of one solve.
 
-    Per round with W_in entries in and W_out kept (both phases):
-      find/min pass:  S*W_in (read) + 2*4*W_in (parent, depth 1) + 2*8*W_in (guard reads)
-                      + S*W_out (compacted write) + 2*8*A (atomicMin)
-                      + 2*8*W_in (reset of the previous round's slots, rounds > 0)
-      mark pass:      S*W_out (read) + 2*8*W_out (min-slot reads)
+    Per round with W_in real entries in and W_out kept (both phases):
+      first round of a phase (in place on the scan's list, no find, no copy):
+                      S*W_in (read) + 2*8*W_in (guard reads), W_out = W_in
+      later rounds:   S*W_in (read) + 2*4*W_in (parent, depth 1) + 2*8*W_in (guard reads)
+                      + S*W_out (compacted write)
+                      + reset of the previous round's slots: 8*n (whole array) when
+                        4*W_in >= n, else 2*8*W_in
+      every round:    2*8*A (atomicMin) + mark pass S*W_out (read) + 2*8*W_out (min-slot reads)
     A = guarded atomics actually issued when counted, else 2*W_out (upper bound).
     """
     total = 0
@@ -158,10 +161,12 @@ def round_kernel_bytes(st, entry_bytes=16, atomics=None):
         for r in range(st["rounds"][p]):
             win = w[r]
             wout = w[r + 1] if r + 1 < len(w) else 0
-            total += entry_bytes * win + 8 * win + 16 * win + entry_bytes * wout
-            total += 16 * wout + entry_bytes * wout
-            if r > 0:
-                total += 16 * win
+            if r == 0:
+                total += entry_bytes * win + 16 * win
+            else:
+                total += entry_bytes * win + 8 * win + 16 * win + entry_bytes * wout
+                total += 8 * nodes if 4 * win >= nodes else 16 * win
+            total += entry_bytes * wout + 16 * wout
     a = atomics if atomics is not None else 2 * sum(
         (wl[p][r + 1] if r + 1 < len(wl[p]) else 0)
         for p in range(2) for r in range(st["rounds"][p]))
@@ -537,7 +542,7 @@ def main():
     d2h = g.edges
 
     peak, peak_kind = load_peaks()
-    rb = round_kernel_bytes(last, atomics=st_atom["atomics"])
+    rb = round_kernel_bytes(last, g.nodes, atomics=st_atom["atomics"])
     sb = scan_kernel_bytes(last, g.nodes, g.edges)
     r_ms = sum(round_ms) / len(round_ms)
     s_ms = sum(scan_ms) / len(scan_ms)
