@@ -625,10 +625,17 @@ __global__ void __launch_bounds__(kScanThreads, ScanCfg<EPT>::kMinBlocks) k_scan
       nrep[q] = nb[q];
     }
     if (KIND == kHeavy) {  // light-tree reps of both endpoints, all loads in flight together
+      // A lane's entries run in CSR order, so consecutive ones mostly share
+      // their row: its rep is loaded once per row, not once per entry.
+      int rv = -1, rrep = 0;
 #pragma unroll
       for (int q = 0; q < EPT; q++)
         if (cand & (1u << q)) {
-          vtx[q] = __ldg(a.parent + vtx[q]);
+          if (vtx[q] != rv) {
+            rv = vtx[q];
+            rrep = __ldg(a.parent + rv);
+          }
+          vtx[q] = rrep;
           nrep[q] = __ldg(a.parent + nb[q]);
         }
 #pragma unroll
