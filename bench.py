@@ -14,7 +14,8 @@ artifact's throughput definition (generate_compare_tables.py:59) in G.
 
 --impl reference times the reference's own CPU implementation of the path,
 cpuMST (serial Kruskal, ECL_MST.cu:82-124) compiled from the reference
-sources (oracle/_ref), on a bounded sample of the workload.
+sources (oracle/_ref), on the same workload graph; that process loads no
+library of this package.
 
 With N > 1 (torchrun) each rank solves its own replica of the graph on its
 GPU (a single graph does not shard: "replicas only"); value = all ranks'
@@ -50,8 +51,6 @@ WORKLOADS = {
     "er16m": ("er", dict(nodes=1 << 24, avg_degree=32, seed=3, wmax=1 << 30),
               "Erdos-Renyi 16,777,216 vertices, avg degree 32, seed 3, w~U[1,2^30]"),
 }
-CPU_SAMPLE = {"rmat22": ("rmat", dict(scale=20, edge_factor=16, seed=2, wmax=1 << 24),
-                         "RMAT scale 20 (same family and parameters, 1/4 of the entries)")}
 
 
 def make_graph(E, kind, kw):
@@ -318,33 +317,65 @@ def preprocess_leg(E, kind, kw, g, gen_s):
             "what": "synchronous ecl_gen_*_device call (wall clock, outputs cudaMalloc'd) vs the host generator"}
 
 
-def reference_arm(args, E):
-    """bench.py --impl reference: the reference's cpuMST on the host cores."""
+def oracle_graph(kind, kw):
+    """The workload drawn by the oracle's generators (oracle/graphgen.c): the
+    same CSR as make_graph's, built without loading the product library."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    if kind == "rmat":
+        return O.gen_rmat(kw["scale"], kw["edge_factor"], RMAT["a"], RMAT["b"], RMAT["c"], kw["seed"], kw["wmax"])
+    if kind == "grid":
+        return O.gen_grid(kw["rows"], kw["cols"], kw["seed"], kw["wmax"])
+    if kind == "er":
+        return O.gen_er(kw["nodes"], kw["avg_degree"], kw["seed"], kw["wmax"])
+    raise ValueError(kind)
+
+
+def reference_arm(args):
+    """bench.py --impl reference: the reference's own CPU implementation of the
+    path, cpuMST (serial Kruskal, ECL_MST.cu:82-124) compiled from the reference
+    sources (oracle/_ref), timed on the host on the same workload graph as the
+    GPU arm. The graph comes from the oracle's generators, so this process
+    loads only the oracle and the reference, never the product library. Where
+    oracle/_ref is absent the oracle's restatement (oracle/kruskal.c) is timed
+    instead and the line says so. Only rank 0 works under torchrun."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as O
 
-    kind, kw, desc = CPU_SAMPLE.get(args.workload, WORKLOADS[args.workload])
-    g = make_graph(E, kind, kw)
+    kind, kw, desc = WORKLOADS[args.workload]
+    t0 = time.perf_counter()
+    nindex, nlist, eweight = oracle_graph(kind, kw)
+    gen_s = time.perf_counter() - t0
+    nodes, edges = len(nindex) - 1, len(nlist)
+    if O.have_ref():
+        run, kind_name = (lambda: O.ref_cpu_mst(nindex, nlist, eweight)), "reference"
+        what = "reference cpuMST (serial Kruskal, ECL_MST.cu:82-124) compiled from the reference sources"
+    else:
+        t, f = O.oracle_heuristic(nodes, eweight)
+        run, kind_name = (lambda: O.oracle_mst(nindex, nlist, eweight, t, f)), "port"
+        what = "the oracle's restatement of cpuMST (oracle/kruskal.c); the reference build is absent"
     times = []
     for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        O.ref_cpu_mst(g.nindex, g.nlist, g.eweight)
-        dt = time.perf_counter() - t0
+        t1 = time.perf_counter()
+        run()
+        dt = time.perf_counter() - t1
         if i >= args.warmup:
             times.append(dt)
     tot = sum(times)
-    value = args.steps * g.edges / tot / 1e9
+    value = args.steps * edges / tot / 1e9
+    sample = f"{what}, 1 thread, on the whole workload graph ({desc}); host has {os.cpu_count()} cores"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gedges/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32/uint64", "data": "synthetic",
-        "config": {"workload": args.workload, "sample": desc, "nodes": g.nodes, "edges": g.edges},
-        "cpu_baseline": {"value": value, "unit": "Gedges/s", "cores": 1, "kind": "reference",
-                         "sample": f"reference cpuMST (serial Kruskal, 1 thread) on {desc}"},
+        "config": {"workload": args.workload, "graph": desc, "nodes": nodes, "edges": edges,
+                   "generated_by": "oracle/graphgen.c (identical to the product generator)",
+                   "gen_s": round(gen_s, 2)},
+        "cpu_baseline": {"value": value, "unit": "Gedges/s", "cores": 1, "kind": kind_name, "sample": sample},
         "e2e": {"value": value, "unit": "Gedges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -372,11 +403,11 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
-    import ecl_mst as E
-
     if args.impl == "reference":
-        reference_arm(args, E)
+        reference_arm(args)
         return
+
+    import ecl_mst as E
 
     import torch
     import torch.distributed as dist

@@ -1,7 +1,9 @@
 """ctypes access to the ORACLE (oracle/liboracle.so, oracle/_ref/libecl_ref.so).
 
 Test infrastructure only: used as the checker by the tests, the smoke check
-and the benchmark's CPU-baseline leg.
+and the benchmark's CPU-baseline and reference legs. Nothing here loads the
+product library, so a process that imports only this module (the
+benchmark's reference arm) maps the oracle and the reference alone.
 """
 import ctypes
 import os
@@ -36,7 +38,48 @@ def oracle():
         _orc.oracle_verify.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.POINTER(ctypes.c_int64)]
         _orc.oracle_synth.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        _orc.gg_rmat.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_double, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(_GG)]
+        _orc.gg_er.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_uint64, ctypes.c_int32,
+                               ctypes.POINTER(_GG)]
+        _orc.gg_grid.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, ctypes.c_int32,
+                                 ctypes.POINTER(_GG)]
+        _orc.gg_free.argtypes = [ctypes.POINTER(_GG)]
     return _orc
+
+
+class _GG(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_int32), ("edges", ctypes.c_int32), ("nindex", ctypes.c_void_p),
+                ("nlist", ctypes.c_void_p), ("eweight", ctypes.c_void_p)]
+
+
+def _take(fn, *args):
+    g = _GG()
+    st = fn(*args, ctypes.byref(g))
+    if st != 0:
+        raise RuntimeError(f"oracle generator failed ({st})")
+    try:
+        def arr(p, count):
+            a = np.empty(count, np.int32)
+            if count:
+                ctypes.memmove(a.ctypes.data, p, 4 * count)
+            return a
+        return arr(g.nindex, g.nodes + 1), arr(g.nlist, g.edges), arr(g.eweight, g.edges)
+    finally:
+        oracle().gg_free(ctypes.byref(g))
+
+
+def gen_rmat(scale, edge_factor, a, b, c, seed, wmax):
+    """(nindex, nlist, eweight) of the seeded RMAT graph (oracle/graphgen.c)."""
+    return _take(oracle().gg_rmat, scale, edge_factor, a, b, c, seed, wmax)
+
+
+def gen_er(nodes, avg_degree, seed, wmax):
+    return _take(oracle().gg_er, nodes, avg_degree, seed, wmax)
+
+
+def gen_grid(rows, cols, seed, wmax):
+    return _take(oracle().gg_grid, rows, cols, seed, wmax)
 
 
 def have_ref():

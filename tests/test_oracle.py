@@ -94,3 +94,22 @@ def test_oracle_synth_wraps_like_int32():
     wrapped = ((prod + 2**31) % 2**32) - 2**31
     r = int(np.fmod(wrapped, n))
     assert int(w[0]) == abs(1 + r)
+
+
+@pytest.mark.parametrize("kind", ["rmat", "er", "grid"])
+def test_oracle_generators_match_library(kind):
+    """The oracle's input generators (oracle/graphgen.c, used by the
+    benchmark's reference arm so that its process loads no product library)
+    draw the same CSR as the library's generators, entry for entry."""
+    import ecl_mst as E
+    if kind == "rmat":
+        want = E.gen_rmat(15, 16, 0.57, 0.19, 0.19, 2, 1 << 24)
+        got = O.gen_rmat(15, 16, 0.57, 0.19, 0.19, 2, 1 << 24)
+    elif kind == "er":
+        want = E.gen_er(20_000, 8, 7, 1 << 20)
+        got = O.gen_er(20_000, 8, 7, 1 << 20)
+    else:
+        want = E.gen_grid(123, 77, 1, 1_000_000)
+        got = O.gen_grid(123, 77, 1, 1_000_000)
+    for a, b in zip(got, (want.nindex, want.nlist, want.eweight)):
+        assert np.array_equal(a, b)
