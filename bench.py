@@ -295,6 +295,57 @@ def device_graph(E, kind, kw):
     raise ValueError(kind)
 
 
+def grid_leg(args, E, torch, dev, mode, flush):
+    """The small plain-method configuration as a sub-record: the 1000x1000
+    4-neighbour grid (seed 1, w~U[1,1e6]; m/n = 3, so the reference runs it
+    unfiltered), drawn on the device, solved with the headline schedule and
+    with the reference heuristic, against the plain ECL-MST on the same GPU."""
+    kind, kw, desc = WORKLOADS["grid1000"]
+    dg = device_graph(E, kind, kw)
+    n, m = dg.nodes, dg.edges
+    out = torch.empty(m, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    res = {"graph": desc, "nodes": n, "edges": m}
+    with E.Context(n, m, device=dev.index or 0) as ctx:
+        for name, md in (("headline_schedule", mode), ("heuristic_schedule", E.THRESH_HEURISTIC)):
+            o = E.make_opts(mode=md)
+            ms = []
+            for i in range(3 + max(5, args.steps // 2)):
+                flush.max()
+                st = ctx.run_device(n, m, dg.d_nindex, dg.d_nlist, dg.d_eweight, out.data_ptr(), opts=o,
+                                    stream=stream, stats=True)
+                if i >= 3:
+                    ms.append(st["ms_total"])
+            t = float(np.mean(ms))
+            res[name] = {"ms": t, "gedges_s": m / (t * 1e-3) / 1e9, "filtered": st["filtered"],
+                         "rounds": st["rounds"]}
+    res["value"] = res["headline_schedule"]["gedges_s"]
+    got = out.cpu().numpy()
+    g = dg.to_host()
+    dg.close()
+    res["forest_weight"] = int(g.eweight[got.astype(bool)].astype(np.int64).sum()) % 2**64
+    plain_so = os.path.join(ROOT, "baseline", "_ref", "libecl_plain.so")
+    if os.path.exists(plain_so) and not args.no_plain:
+        import ctypes
+        lib = ctypes.CDLL(plain_so)
+        P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        f, th = ctypes.c_int(), ctypes.c_int()
+        lib.plain_threshold(g.nodes, g.edges, P(g.eweight), ctypes.byref(f), ctypes.byref(th))
+        pout = np.zeros(m, np.uint8)
+        secs = []
+        for _ in range(5):
+            sec = ctypes.c_double()
+            lib.plain_gpu_mst(g.nodes, g.edges, P(g.nindex), P(g.nlist), P(g.eweight), f, th, P(pout),
+                              ctypes.byref(sec))
+            secs.append(sec.value)
+        med = statistics.median(secs[1:])
+        res["plain"] = {"ms": med * 1e3, "gedges_s": m / med / 1e9, "filtered": f.value,
+                        "inMST_identical": bool(np.array_equal(pout, got)),
+                        "what": "reference gpuMST rebuilt for sm_100a, its own timed window, median"}
+        res["vs_plain"] = res["value"] / res["plain"]["gedges_s"]
+    return res
+
+
 def preprocess_leg(E, kind, kw, g, gen_s):
     """GPU-side preprocessing: the workload's graph drawn on the device (pair
     sampling, radix sort of both directions, dedup, CSR emit) against the host
@@ -394,10 +445,11 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain ECL-MST comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-ablation", action="store_true", help="skip the technique-ablation leg")
-    ap.add_argument("--batch", type=int, default=256,
+    ap.add_argument("--batch", type=int, default=4096,
                     help="graphs of the mixed batch to solve in batched mode (0 = skip)")
-    ap.add_argument("--batch-gen", choices=["host", "device"], default="host",
+    ap.add_argument("--batch-gen", choices=["host", "device"], default="device",
                     help="draw the batch with the host generators or on the device (same graphs)")
+    ap.add_argument("--no-grid", action="store_true", help="skip the 1000x1000 grid sub-record")
     ap.add_argument("--profile", action="store_true",
                     help="device solves only (no e2e, plain or CPU legs): the command profiled by ncu")
     args = ap.parse_args()
@@ -457,7 +509,7 @@ def main():
     # correctness of the timed configuration against the oracle-free invariant:
     # forest weight is recomputed on the host from inMST below (exact check in tests)
 
-    step_ms, scan_ms, round_ms, light_us, heavy_us = [], [], [], [], []
+    step_ms, scan_ms, round_ms, light_us, heavy_us, bd_last = [], [], [], [], [], []
     last = None
     if world > 1:
         dist.barrier()
@@ -483,6 +535,7 @@ def main():
             light_us.append(st["us_scan"][0][2])
             heavy_us.append(st["us_scan"][1][2])
             last = st
+            bd_last.append(st)
     if world > 1:
         dist.barrier()
     clocks = clk.summary()
@@ -595,10 +648,24 @@ def main():
     if os.path.exists(tpath):
         with open(tpath) as f:
             traffic = json.load(f).get(args.workload, {}).get(dom)
+    for k in ("rounds", "scan"):
+        kernels[k]["frac"] = kernels[k]["gbs"] / peak
+    # whole-solve lower bound: nindex + nlist + eweight read once, inMST written once
+    b_run = 9 * g.edges + 4 * g.nodes + 4
+    run = {"bytes": b_run, "ms": ms_step, "gbs": b_run / (ms_step * 1e-3) / 1e9,
+           "frac": b_run / (ms_step * 1e-3) / 1e9 / peak,
+           "what": "9m + 4n + 4 bytes (CSR read once, inMST written once) over the whole solve"}
     roofline = {"bound": "hbm", "kernel": "k_rounds (both phases)" if dom == "rounds" else "k_scan (light+heavy)",
                 "achieved": kernels[dom]["gbs"], "peak": peak, "unit": "GB/s",
                 "frac": kernels[dom]["gbs"] / peak, "peak_source": peak_kind, "traffic": traffic,
-                "per_kernel": kernels}
+                "per_kernel": kernels, "run": run}
+    # per-round attribution of the round kernel (device timestamps, direct-launch solves)
+    rounds_detail = []
+    for p_ in range(2):
+        for r_ in range(last["rounds"][p_]):
+            us = np.mean([np.array(x["us_round"][p_][r_]) for x in bd_last], axis=0)
+            rounds_detail.append({"phase": p_, "round": r_, "entries": last["wl_real"][p_][r_],
+                                  "us_find_min": round(float(us[0]), 1), "us_mark": round(float(us[1]), 1)})
 
     # the plain form: the reference ECL_MST.cu rebuilt for sm_100a, same graph, same GPU
     plain = None
@@ -626,6 +693,10 @@ def main():
         # one GPU: the whole batch; several: each rank its shard of the graphs (shard.py)
         batch = batch_leg(args, E, torch, dev, rank, world, dist if world > 1 else None)
 
+    grid = None
+    if rank == 0 and not args.no_grid and world == 1:
+        grid = grid_leg(args, E, torch, dev, mode, flush)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -638,6 +709,32 @@ def main():
                    "sample": f"reference cpuMST (serial Kruskal) on the full workload, {dt:.1f} s, "
                              f"host has {os.cpu_count()} cores",
                    "inMST_identical": bool(np.array_equal(ref_out, inmst))}
+
+    # L2 persistence A/B (ECL_FLAG_L2_PERSIST) with the headline schedule and
+    # direct launches; persisting lines are returned to normal before each
+    # step's L2 flush, so both sides start from a flushed L2. Run last: the
+    # persisting set-aside stays raised until the context is closed.
+    l2ab = None
+    if not args.profile and not args.no_ablation:
+        l2ab = {}
+        for name, extra in (("off", 0), ("on", E.FLAG_L2_PERSIST)):
+            o = E.make_opts(mode=mode, quantile=args.quantile, degree_split=args.split,
+                            flags=E.FLAG_NO_GRAPH | extra)
+            rows = []
+            for i in range(2 + max(5, args.steps // 4)):
+                ctx.l2_reset()
+                flush.max()
+                st_l = ctx.run_device(g.nodes, g.edges, d_ni.data_ptr(), d_nl.data_ptr(), d_ew.data_ptr(),
+                                      d_out.data_ptr(), opts=o, stream=stream.cuda_stream, stats=True)
+                if i >= 2:
+                    rows.append(st_l)
+            l2ab[name] = {"ms": float(np.mean([r["ms_total"] for r in rows])),
+                          "ms_rounds": float(np.mean([r["ms_rounds"] for r in rows])),
+                          "us_light_scan": float(np.mean([r["us_scan"][0][2] for r in rows])),
+                          "us_heavy_scan": float(np.mean([r["us_scan"][1][2] for r in rows])),
+                          "inMST_identical": bool(np.array_equal(d_out[: g.edges].cpu().numpy(), inmst))}
+        l2ab["speedup"] = l2ab["off"]["ms"] / l2ab["on"]["ms"]
+        ctx.l2_reset()
 
     if rank == 0:
         line = {
@@ -662,9 +759,12 @@ def main():
                                     "what": "same solve with the reference threshold heuristic"}
                                    if heur_ms else None),
             "roofline": roofline,
+            "rounds_detail": rounds_detail,
+            "l2_persist": l2ab,
             "cpu_baseline": cpu,
             "plain_ecl_mst": plain,
             "batch": batch,
+            "grid1000": grid,
             "preprocess": preprocess,
             "vs_plain": (value / plain["value"]) if plain else None,
             "forest_weight": fw,

@@ -300,11 +300,16 @@ int ecl_mst_run_device(ecl_mst_ctx* ctx, const ecl_graph* d_graph,
  * every GPU loading this library holds until the process exits.
  *   - d_graph holds DEVICE pointers, d_inMST a device buffer of edges bytes;
  *   - limits: nodes <= 262,144 and edges <= 1,048,576, else ECL_ERR_TOO_LARGE;
- *     at most edges/2 one-direction entries (nlist[j] > v), which every
- *     symmetric input satisfies, else ECL_ERR_OVERFLOW;
- *   - ECL_THRESH_LEARNED is not available here (ECL_ERR_UNSUPPORTED);
+ *     the worklists hold 524,288 entries, enough for every symmetric input
+ *     (at most edges/2 one-direction entries nlist[j] > v); an input with
+ *     more one-direction entries than that returns ECL_ERR_OVERFLOW;
+ *   - ECL_THRESH_LEARNED takes the reference heuristic here, as
+ *     ecl_mst_run_device does for graphs below its learned-schedule cut-off
+ *     (the feature pass needs scratch this entry point does not hold);
  *   - the first call on a device resolves the scratch address on that device
- *     (make it before any stream capture); the call enqueues on `stream`
+ *     (make it before any stream capture) and keeps it for the life of the
+ *     process: do not call it again on a device after cudaDeviceReset, which
+ *     unloads the module that owns the array; the call enqueues on `stream`
  *     (cudaStream_t, NULL = legacy default stream) and returns after the solve
  *     finished, with device-side errors as its status;
  *   - all calls share the one scratch array: calls that overlap on the GPU
@@ -419,6 +424,12 @@ int ecl_mst_ctx_sync(ecl_mst_ctx* ctx);
 
 /* The stream the context enqueues on (a cudaStream_t). */
 void* ecl_mst_ctx_stream(ecl_mst_ctx* ctx);
+
+/* Returns every L2 line a solve with ECL_FLAG_L2_PERSIST marked persisting to
+ * normal status (cudaCtxResetPersistingL2Cache on the context's device), so
+ * later traffic can evict them. No counterpart in the reference, which sets
+ * no L2 policy. */
+int ecl_mst_ctx_l2_reset(ecl_mst_ctx* ctx);
 
 /* Pinned host memory for fast H2D/D2H (cudaHostAlloc / cudaFreeHost). */
 int ecl_host_alloc_pinned(size_t bytes, void** out);

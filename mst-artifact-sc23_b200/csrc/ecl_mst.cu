@@ -37,11 +37,16 @@ struct ecl_mst_ctx {
   // the last solve's key, and the captured solve (CUDA graph) with its key
   std::vector<long long> last_key, exec_key;
   cudaGraphExec_t exec = nullptr;
-  // [minv0 | minv1 | parent] in one allocation (one L2 access-policy window)
+  // [minv0 | minv1 | parent] in one allocation, laid out per solve for the
+  // graph's vertex count (minv0 = slots, minv1 = minv0 + n, parent after
+  // minv1), so one L2 access-policy window covers exactly the 20n bytes used
   void* slots = nullptr;
-  int* parent = nullptr;
-  u64* minv0 = nullptr;
-  u64* minv1 = nullptr;
+  // L2 persistence (ECL_FLAG_L2_PERSIST): the device's persisting set-aside
+  // and window limits, and the set-aside this context raised (restored at
+  // destroy)
+  size_t l2_persist_max = 0, l2_window_max = 0;
+  size_t l2_limit_prev = 0;
+  bool l2_limit_set = false;
   int4* wl[2] = {nullptr, nullptr};
   unsigned wl_cap = 0;
   int* first_v = nullptr;  // tile -> vertex table of the edge-balanced scans
@@ -96,6 +101,50 @@ int coop_grid(const void* fn, int threads, int sm_count) {
   return per_sm * sm_count;
 }
 
+// The solve's slot arrays inside ctx->slots, packed for n vertices.
+struct Slots {
+  u64* minv0;
+  u64* minv1;
+  int* parent;
+  size_t bytes;  // 20n
+};
+Slots slots_for(void* base, int n) {
+  Slots sl;
+  sl.minv0 = (u64*)base;
+  sl.minv1 = sl.minv0 + n;
+  sl.parent = (int*)(sl.minv1 + n);
+  sl.bytes = (size_t)n * (2 * sizeof(u64) + sizeof(int));
+  return sl;
+}
+
+// Launch `kernel` with optional launch attributes: cooperative (grid-wide
+// barriers) and an L2 access-policy window. Without either it is a plain
+// launch.
+template <typename... KArgs, typename... Args>
+int launch_ex(void (*kernel)(KArgs...), int grid, int threads, size_t smem, cudaStream_t s, bool coop,
+              const cudaAccessPolicyWindow* win, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[2];
+  unsigned na = 0;
+  if (coop) {
+    at[na].id = cudaLaunchAttributeCooperative;
+    at[na].val.cooperative = 1;
+    na++;
+  }
+  if (win) {
+    at[na].id = cudaLaunchAttributeAccessPolicyWindow;
+    at[na].val.accessPolicyWindow = *win;
+    na++;
+  }
+  cfg.attrs = na ? at : nullptr;
+  cfg.numAttrs = na;
+  return cuda_status(cudaLaunchKernelEx(&cfg, kernel, args...));
+}
+
 int prepare_scan_kernels();
 
 // Entries of the tile->vertex table buffer for up to `edges` CSR entries: the
@@ -107,10 +156,15 @@ int64_t first_v_entries(int64_t edges) {
 
 // k_prep, then the fill scan that completes the tile->vertex table
 // (first_v: pa.tiles + 1 entries, then room for the chunk maxima).
-int enqueue_prep(const PrepArgs& pa, int sm_count, cudaStream_t s) {
+int enqueue_prep(const PrepArgs& pa, int sm_count, cudaStream_t s, const cudaAccessPolicyWindow* win = nullptr) {
   ECL_CUDA_TRY(cudaMemsetAsync(pa.first_v, 0, sizeof(int) * (size_t)pa.tiles, s));
   const int prep_grid = (int)std::min<int64_t>((pa.nodes + kThreads - 1) / kThreads, (int64_t)sm_count * 16);
-  k_prep<<<std::max(prep_grid, 1), kThreads, 0, s>>>(pa);
+  if (win) {
+    int st = launch_ex(k_prep, std::max(prep_grid, 1), kThreads, 0, s, false, win, pa);
+    if (st) return st;
+  } else {
+    k_prep<<<std::max(prep_grid, 1), kThreads, 0, s>>>(pa);
+  }
   const int chunks = (pa.tiles + kFillChunk - 1) / kFillChunk;
   int* chunk_max = pa.first_v + pa.tiles + 1;
   k_fill_chunks<<<chunks, 1024, 0, s>>>(pa.first_v, pa.tiles, chunk_max);
@@ -162,9 +216,8 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   if ((st = cuda_status(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming)))) return fail(st);
   const size_t slot_bytes = (size_t)max_nodes * (2 * sizeof(u64) + sizeof(int));
   if ((st = cuda_status(cudaMalloc(&c->slots, slot_bytes)))) return fail(st);
-  c->minv0 = (u64*)c->slots;
-  c->minv1 = c->minv0 + max_nodes;
-  c->parent = (int*)(c->minv1 + max_nodes);
+  c->l2_persist_max = prop.persistingL2CacheMaxSize > 0 ? (size_t)prop.persistingL2CacheMaxSize : 0;
+  c->l2_window_max = prop.accessPolicyMaxWindowSize > 0 ? (size_t)prop.accessPolicyMaxWindowSize : 0;
   // A phase's worklist holds at most one entry per one-direction CSR entry,
   // i.e. at most `edges` (the reference sizes it edges/2, :279, which only
   // holds for symmetric inputs), plus slack for the unused tails of the
@@ -194,6 +247,10 @@ extern "C" void ecl_mst_ctx_destroy(ecl_mst_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->l2_limit_set) {  // hand the persisting set-aside back as it was
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, c->l2_limit_prev);
+  }
   cudaFree(c->slots);
   cudaFree(c->wl[0]);
   cudaFree(c->wl[1]);
@@ -220,6 +277,13 @@ extern "C" void ecl_mst_ctx_destroy(ecl_mst_ctx* c) {
 }
 
 extern "C" void* ecl_mst_ctx_stream(ecl_mst_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+extern "C" int ecl_mst_ctx_l2_reset(ecl_mst_ctx* c) {
+  if (!c) return ECL_ERR_INVALID_ARG;
+  ECL_CUDA_TRY(cudaSetDevice(c->device));
+  ECL_CUDA_TRY(cudaCtxResetPersistingL2Cache());
+  return ECL_OK;
+}
 
 extern "C" int ecl_mst_ctx_sync(ecl_mst_ctx* c) {
   if (!c) return ECL_ERR_INVALID_ARG;
@@ -253,7 +317,7 @@ int prepare_scan_kernels() {
 // warps' slot chunk is sized so that the unused chunk tails (at most
 // chunk - 1 per warp) fit in the worklist's slack.
 template <int KIND, int EPT>
-int launch_scan_ept(const ScanArgs& sa, cudaStream_t s) {
+int launch_scan_ept(const ScanArgs& sa, cudaStream_t s, const cudaAccessPolicyWindow* win) {
   const int64_t m = sa.edges;
   const int64_t tile = ScanCfg<EPT>::kTile;
   const int tiles = (int)((m + tile - 1) / tile);
@@ -264,26 +328,48 @@ int launch_scan_ept(const ScanArgs& sa, cudaStream_t s) {
   ScanArgs a = sa;
   const int64_t warps = (int64_t)blocks * kScanWarps;
   a.chunk = (unsigned)std::max<int64_t>(1, std::min<int64_t>(kScanMaxChunk, (int64_t)sa.wl_slack / warps));
+  if (win) return launch_ex(k_scan<KIND, EPT>, blocks, kScanThreads, scan_smem_bytes<EPT>(), s, false, win, a);
   k_scan<KIND, EPT><<<blocks, kScanThreads, scan_smem_bytes<EPT>(), s>>>(a);
   return cuda_status(cudaGetLastError());
 }
 
 template <int KIND>
-int launch_scan(int ept, const ScanArgs& sa, cudaStream_t s) {
-  if (ept == 4) return launch_scan_ept<KIND, 4>(sa, s);
-  if (ept == 8) return launch_scan_ept<KIND, 8>(sa, s);
-  return launch_scan_ept<KIND, 16>(sa, s);
+int launch_scan(int ept, const ScanArgs& sa, cudaStream_t s, const cudaAccessPolicyWindow* win = nullptr) {
+  if (ept == 4) return launch_scan_ept<KIND, 4>(sa, s, win);
+  if (ept == 8) return launch_scan_ept<KIND, 8>(sa, s, win);
+  return launch_scan_ept<KIND, 16>(sa, s, win);
 }
 
 // Scan variants to launch: the one the split selects, or all three (each
 // exits unless st->split selects it) when the split is chosen on the device.
 template <int KIND>
-int launch_scans(bool device_split, int split, const ScanArgs& sa, cudaStream_t s) {
-  if (!device_split) return launch_scan<KIND>(scan_ept(split), sa, s);
+int launch_scans(bool device_split, int split, const ScanArgs& sa, cudaStream_t s,
+                 const cudaAccessPolicyWindow* win) {
+  if (!device_split) return launch_scan<KIND>(scan_ept(split), sa, s, win);
   int st;
   for (int ept : {4, 8, 16})
-    if ((st = launch_scan<KIND>(ept, sa, s))) return st;
+    if ((st = launch_scan<KIND>(ept, sa, s, win))) return st;
   return ECL_OK;
+}
+
+// The L2 access-policy window of a solve (ECL_FLAG_L2_PERSIST): the packed
+// min-slot and parent arrays (20n bytes; the min slots alone when the window
+// limit is smaller), with the share of lines the persisting set-aside can
+// hold marked persisting and the rest left normal.
+bool l2_window(const ecl_mst_ctx* c, const Slots& sl, bool parent_only, cudaAccessPolicyWindow* w) {
+  if (!c->l2_limit_set || c->l2_window_max == 0) return false;
+  memset(w, 0, sizeof(*w));
+  w->base_ptr = parent_only ? (void*)sl.parent : (void*)sl.minv0;
+  size_t bytes = parent_only ? (sl.bytes / 5) : sl.bytes;  // parent is 4n of the 20n
+  bytes = std::min(bytes, c->l2_window_max);
+  if (bytes == 0) return false;
+  w->num_bytes = bytes;
+  size_t persist = 0;
+  cudaDeviceGetLimit(&persist, cudaLimitPersistingL2CacheSize);
+  w->hitRatio = (float)std::min(1.0, (double)persist / (double)bytes);
+  w->hitProp = cudaAccessPropertyPersisting;
+  w->missProp = cudaAccessPropertyStreaming;
+  return true;
 }
 
 // `join`, when set, is recorded on the stream that runs the learned
@@ -294,14 +380,21 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   const int split = o->degree_split > 0 ? o->degree_split : kDefaultSplit;
   const bool device_split = o->threshold_mode == ECL_THRESH_LEARNED;
   const int tiles = (int)(((int64_t)m + kGran - 1) / kGran);
+  const Slots sl = slots_for(c->slots, n);
+  // L2 persistence: k_prep writes the slots and parent, the rounds hammer
+  // them, the flatten pass and the heavy scan gather parent[]
+  cudaAccessPolicyWindow w_all, w_par;
+  const bool l2 = (o->flags & ECL_FLAG_L2_PERSIST) != 0;
+  const cudaAccessPolicyWindow* win_all = l2 && l2_window(c, sl, false, &w_all) ? &w_all : nullptr;
+  const cudaAccessPolicyWindow* win_par = l2 && l2_window(c, sl, true, &w_par) ? &w_par : nullptr;
   PrepArgs pa;
   pa.nodes = n;
   pa.edges = m;
   pa.nindex = g->nindex;
   pa.eweight = g->eweight;
-  pa.parent = c->parent;
-  pa.minv0 = c->minv0;
-  pa.minv1 = c->minv1;
+  pa.parent = sl.parent;
+  pa.minv0 = sl.minv0;
+  pa.minv1 = sl.minv1;
   pa.first_v = c->first_v;
   pa.tiles = tiles;
   pa.mode = o->threshold_mode;
@@ -310,7 +403,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   pa.quantile = o->quantile;
   pa.st = c->st;
   int st;
-  if ((st = enqueue_prep(pa, c->sm_count, s))) return st;
+  if ((st = enqueue_prep(pa, c->sm_count, s, win_all))) return st;
   if (join) ECL_CUDA_TRY(cudaStreamWaitEvent(s, join, 0));
   ScanArgs sa;
   sa.nodes = n;
@@ -320,7 +413,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   sa.eweight = g->eweight;
   sa.first_v = c->first_v;
   sa.tiles = tiles;
-  sa.parent = c->parent;
+  sa.parent = sl.parent;
   sa.wl = c->wl[0];
   sa.wl_cap = c->wl_cap;
   sa.wl_slack = c->wl_cap - (unsigned)m;  // a scan keeps at most m entries
@@ -334,9 +427,9 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   ra.wl0 = c->wl[0];
   ra.wl1 = c->wl[1];
   ra.wl_cap = c->wl_cap;
-  ra.parent = c->parent;
-  ra.minv0 = c->minv0;
-  ra.minv1 = c->minv1;
+  ra.parent = sl.parent;
+  ra.minv0 = sl.minv0;
+  ra.minv1 = sl.minv1;
   ra.inMST = d_inMST;
   ra.st = c->st;
   ra.small_tail = o->small_tail < 0 ? 0u : (o->small_tail == 0 ? kDefaultSmallTail : (unsigned)o->small_tail);
@@ -345,19 +438,29 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   ra.abl = round_ablation(o->flags);
   const int rgrid = std::max(1, std::min(c->round_grid, (m / 2 + kRoundThreads - 1) / kRoundThreads + 1));
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[5], s));
-  if ((st = launch_scans<kLight>(device_split, split, sa, s))) return st;
+  if ((st = launch_scans<kLight>(device_split, split, sa, s, nullptr))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   ra.phase = 0;
-  if ((st = launch_coop((const void*)k_rounds, rgrid, kRoundThreads, &ra, s))) return st;
+  if (win_all) st = launch_ex(k_rounds, rgrid, kRoundThreads, 0, s, true, win_all, ra);
+  else st = launch_coop((const void*)k_rounds, rgrid, kRoundThreads, &ra, s);
+  if (st) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[2], s));
   const int fgrid = (int)std::min<int64_t>(((int64_t)n + kThreads - 1) / kThreads, (int64_t)c->sm_count * 16);
-  k_flatten<<<std::max(fgrid, 1), kThreads, 0, s>>>(c->parent, n, c->st);
-  ECL_CUDA_TRY(cudaGetLastError());
+  if (win_par) {
+    if ((st = launch_ex(k_flatten, std::max(fgrid, 1), kThreads, 0, s, false, win_par, sl.parent, n,
+                        (const DevState*)c->st)))
+      return st;
+  } else {
+    k_flatten<<<std::max(fgrid, 1), kThreads, 0, s>>>(sl.parent, n, c->st);
+    ECL_CUDA_TRY(cudaGetLastError());
+  }
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[6], s));
-  if ((st = launch_scans<kHeavy>(device_split, split, sa, s))) return st;
+  if ((st = launch_scans<kHeavy>(device_split, split, sa, s, win_par))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[3], s));
   ra.phase = 1;
-  if ((st = launch_coop((const void*)k_rounds, rgrid, kRoundThreads, &ra, s))) return st;
+  if (win_all) st = launch_ex(k_rounds, rgrid, kRoundThreads, 0, s, true, win_all, ra);
+  else st = launch_coop((const void*)k_rounds, rgrid, kRoundThreads, &ra, s);
+  if (st) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[4], s));
   return ECL_OK;
 }
@@ -472,6 +575,17 @@ extern "C" int ecl_mst_run_device(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d
   if (o.threshold_mode == ECL_THRESH_LEARNED && (g->edges < kLearnedMinEdges || !ecl_learned_has_weights()))
     o.threshold_mode = ECL_THRESH_HEURISTIC;
   const bool timed = stats != nullptr;
+  if (o.flags & ECL_FLAG_L2_PERSIST) {
+    // Persisting set-aside for this process's context, sized for the solve's
+    // slot arrays (20n bytes) up to the device maximum; set before any
+    // capture, restored when the context is destroyed.
+    const size_t want = std::min(c->l2_persist_max, (size_t)g->nodes * (2 * sizeof(u64) + sizeof(int)));
+    size_t cur = 0;
+    ECL_CUDA_TRY(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
+    if (!c->l2_limit_set) c->l2_limit_prev = cur;
+    if (want > cur) ECL_CUDA_TRY(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
+    c->l2_limit_set = want > 0 || c->l2_limit_set;
+  }
   // inner_events: the per-phase timing events (not inside a captured graph)
   auto enqueue_all = [&](cudaStream_t q, bool inner_events) -> int {
     ECL_CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevState), q));
@@ -690,7 +804,10 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   else ecl_default_opts(&o);
   int st = check_opts(&o);
   if (st) return st;
-  if (o.threshold_mode == ECL_THRESH_LEARNED) return ECL_ERR_UNSUPPORTED;
+  // The learned schedule's feature pass needs scratch this entry point does
+  // not hold; it takes the reference heuristic, as ecl_mst_run_device does
+  // below its learned-schedule cut-off.
+  if (o.threshold_mode == ECL_THRESH_LEARNED) o.threshold_mode = ECL_THRESH_HEURISTIC;
   if (g->edges == 0) return ECL_OK;
   int dev = 0;
   ECL_CUDA_TRY(cudaGetDevice(&dev));

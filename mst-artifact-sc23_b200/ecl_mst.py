@@ -127,6 +127,7 @@ def load():
         "ecl_mst_ctx_sync": (c_int, [c_void_p]),
         "ecl_mst_run_device_noalloc": (c_int, [G, c_void_p, POINTER(MstOpts), c_void_p]),
         "ecl_mst_ctx_stream": (c_void_p, [c_void_p]),
+        "ecl_mst_ctx_l2_reset": (c_int, [c_void_p]),
         "ecl_host_alloc_pinned": (c_int, [ctypes.c_size_t, POINTER(c_void_p)]),
         "ecl_host_free_pinned": (None, [c_void_p]),
         "ecl_batch_ctx_create": (c_int, [c_int, c_int32, c_int64, c_int64, c_int32, POINTER(c_void_p)]),
@@ -524,6 +525,10 @@ class Context:
 
     def sync(self):
         _check(self._lib.ecl_mst_ctx_sync(self.handle), "ctx_sync")
+
+    def l2_reset(self):
+        """Return L2 lines marked persisting (FLAG_L2_PERSIST) to normal."""
+        _check(self._lib.ecl_mst_ctx_l2_reset(self.handle), "ctx_l2_reset")
 
 
 class Batch:
