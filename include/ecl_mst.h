@@ -286,7 +286,14 @@ int ecl_mst_ctx_run_host(ecl_mst_ctx* ctx, const ecl_graph* g, uint8_t* inMST,
  * buffer of edges bytes. Enqueued on `stream` (cudaStream_t, NULL = the
  * context's stream); returns after enqueueing unless stats != NULL, in which
  * case it synchronises and fills stats. Errors found on the device are
- * returned by ecl_mst_ctx_sync. */
+ * returned by ecl_mst_ctx_sync.
+ * A context's worklists start at the size a symmetric input needs (edges/2
+ * one-direction entries nlist[j] > v, as the reference sizes them,
+ * ECL_MST.cu:279, plus slack). An input with more one-direction entries
+ * overflows them; the library then grows them to hold every CSR entry and
+ * solves again, inside this call when stats != NULL, else inside
+ * ecl_mst_ctx_sync, which must therefore be called before inMST is read
+ * when the input may not be symmetric. */
 int ecl_mst_run_device(ecl_mst_ctx* ctx, const ecl_graph* d_graph,
                        uint8_t* d_inMST, const mst_opts* opts, void* stream,
                        ecl_mst_stats* stats);

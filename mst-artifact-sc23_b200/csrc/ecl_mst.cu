@@ -49,6 +49,18 @@ struct ecl_mst_ctx {
   bool l2_limit_set = false;
   int4* wl[2] = {nullptr, nullptr};
   unsigned wl_cap = 0;
+  // false: each list holds max_edges / 2 entries plus slack (every symmetric
+  // input); true: max_edges plus slack (any input). A solve whose scan
+  // overflows the half-size lists is repeated after they are grown.
+  bool wl_full = false;
+  // the last device solve, kept so ecl_mst_ctx_sync can repeat it after a
+  // worklist overflow
+  bool pending = false;
+  ecl_graph pend_graph = {};
+  unsigned char* pend_out = nullptr;
+  mst_opts pend_opts = {};
+  cudaStream_t pend_stream = nullptr;
+  bool resolved = false;  // the last ecl_mst_ctx_sync repeated the solve
   int* first_v = nullptr;  // tile -> vertex table of the edge-balanced scans
   int first_v_cap = 0;
   DevState* st = nullptr;
@@ -180,6 +192,28 @@ unsigned round_ablation(int flags) {
 
 }  // namespace
 
+namespace {
+
+// A phase's worklist holds one entry per one-direction CSR entry
+// (nlist[j] > v) at most. That is edges / 2 for a symmetric input (the size
+// the reference gives it, ECL_MST.cu:279) and up to `edges` otherwise; the
+// lists start at the symmetric size and grow to the full one when a solve
+// overflows them. Both carry slack for the unused tails of the scan warps'
+// slot chunks.
+int alloc_worklists(ecl_mst_ctx* c, bool full) {
+  cudaFree(c->wl[0]);
+  cudaFree(c->wl[1]);
+  c->wl[0] = c->wl[1] = nullptr;
+  const int64_t keep = full ? c->max_edges : c->max_edges / 2;
+  c->wl_cap = (unsigned)std::max<int64_t>(keep + std::min<int64_t>(c->max_edges, kWlSlack), 1);
+  c->wl_full = full;
+  for (int i = 0; i < 2; i++)
+    ECL_CUDA_TRY(cudaMalloc(&c->wl[i], (size_t)c->wl_cap * sizeof(int4)));
+  return ECL_OK;
+}
+
+}  // namespace
+
 extern "C" void ecl_default_opts(mst_opts* o) {
   if (!o) return;
   memset(o, 0, sizeof(*o));
@@ -218,13 +252,7 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   if ((st = cuda_status(cudaMalloc(&c->slots, slot_bytes)))) return fail(st);
   c->l2_persist_max = prop.persistingL2CacheMaxSize > 0 ? (size_t)prop.persistingL2CacheMaxSize : 0;
   c->l2_window_max = prop.accessPolicyMaxWindowSize > 0 ? (size_t)prop.accessPolicyMaxWindowSize : 0;
-  // A phase's worklist holds at most one entry per one-direction CSR entry,
-  // i.e. at most `edges` (the reference sizes it edges/2, :279, which only
-  // holds for symmetric inputs), plus slack for the unused tails of the
-  // scan warps' slot chunks.
-  c->wl_cap = (unsigned)std::max<int64_t>(max_edges + std::min<int64_t>(max_edges, kWlSlack), 1);
-  for (int i = 0; i < 2; i++)
-    if ((st = cuda_status(cudaMalloc(&c->wl[i], (size_t)c->wl_cap * sizeof(int4))))) return fail(st);
+  if ((st = alloc_worklists(c, false))) return fail(st);
   c->first_v_cap = (int)first_v_entries(max_edges);
   if ((st = cuda_status(cudaMalloc(&c->first_v, (size_t)c->first_v_cap * sizeof(int))))) return fail(st);
   if ((st = cuda_status(cudaMalloc(&c->st, sizeof(DevState))))) return fail(st);
@@ -285,12 +313,33 @@ extern "C" int ecl_mst_ctx_l2_reset(ecl_mst_ctx* c) {
   return ECL_OK;
 }
 
+namespace {
+int run_device_once(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d_inMST, const mst_opts* opts, void* stream,
+                    ecl_mst_stats* stats);
+int grow_worklists(ecl_mst_ctx* c);
+}  // namespace
+
 extern "C" int ecl_mst_ctx_sync(ecl_mst_ctx* c) {
   if (!c) return ECL_ERR_INVALID_ARG;
   ECL_CUDA_TRY(cudaSetDevice(c->device));
-  ECL_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->resolved = false;
+  cudaStream_t s = c->pending ? c->pend_stream : c->stream;
+  ECL_CUDA_TRY(cudaStreamSynchronize(s));
+  if (s != c->stream) ECL_CUDA_TRY(cudaStreamSynchronize(c->stream));
   unsigned err = 0;
   ECL_CUDA_TRY(cudaMemcpy(&err, &c->st->error, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if ((err & kErrOverflow) && c->pending && !c->wl_full) {
+    // the input had more one-direction entries than half its CSR entries:
+    // solve it again with worklists that hold every entry
+    c->pending = false;
+    int st = grow_worklists(c);
+    if (st) return st;
+    if ((st = run_device_once(c, &c->pend_graph, c->pend_out, &c->pend_opts, c->pend_stream, nullptr))) return st;
+    c->resolved = true;
+    ECL_CUDA_TRY(cudaStreamSynchronize(c->pend_stream));
+    ECL_CUDA_TRY(cudaMemcpy(&err, &c->st->error, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  }
+  c->pending = false;
   return device_error_status(err);
 }
 
@@ -416,7 +465,9 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   sa.parent = sl.parent;
   sa.wl = c->wl[0];
   sa.wl_cap = c->wl_cap;
-  sa.wl_slack = c->wl_cap - (unsigned)m;  // a scan keeps at most m entries
+  // a scan keeps at most m entries, m / 2 for the symmetric input the
+  // half-size lists assume (more overflows, and the solve is repeated)
+  sa.wl_slack = c->wl_cap - (unsigned)(c->wl_full ? m : m / 2);
   sa.inMST = d_inMST;
   sa.vec_ok = ((((uintptr_t)g->nlist) | ((uintptr_t)g->eweight)) & 15) == 0;
   sa.zero_vec = (((uintptr_t)d_inMST) & 15) == 0;
@@ -552,8 +603,10 @@ int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, float** feat, void**
   return ECL_OK;
 }
 
-extern "C" int ecl_mst_run_device(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d_inMST,
-                                  const mst_opts* opts, void* stream, ecl_mst_stats* stats) {
+namespace {
+
+int run_device_once(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d_inMST, const mst_opts* opts, void* stream,
+                    ecl_mst_stats* stats) {
   int st = check_graph_args(c, g, d_inMST);
   if (st) return st;
   mst_opts o;
@@ -663,6 +716,47 @@ extern "C" int ecl_mst_run_device(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d
   return ECL_OK;
 }
 
+// Worklists grown to hold every CSR entry; the captured solve refers to the
+// old lists and is dropped.
+int grow_worklists(ecl_mst_ctx* c) {
+  ECL_CUDA_TRY(cudaSetDevice(c->device));
+  ECL_CUDA_TRY(cudaDeviceSynchronize());
+  if (c->exec) {
+    cudaGraphExecDestroy(c->exec);
+    c->exec = nullptr;
+  }
+  c->exec_key.clear();
+  c->last_key.clear();
+  return alloc_worklists(c, true);
+}
+
+}  // namespace
+
+extern "C" int ecl_mst_run_device(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d_inMST,
+                                  const mst_opts* opts, void* stream, ecl_mst_stats* stats) {
+  int st = run_device_once(c, g, d_inMST, opts, stream, stats);
+  if (!c) return st;
+  if (stats) {
+    // The solve has finished: an input with more one-direction entries than
+    // the half-size worklists hold is solved again with full-size ones.
+    c->pending = false;
+    if (st == ECL_ERR_OVERFLOW && !c->wl_full && (c->st_host->error & kErrOverflow)) {
+      if ((st = grow_worklists(c))) return st;
+      st = run_device_once(c, g, d_inMST, opts, stream, stats);
+    }
+    return st;
+  }
+  if (st == ECL_OK) {  // enqueued: ecl_mst_ctx_sync checks it and repeats it on overflow
+    c->pending = true;
+    c->pend_graph = *g;
+    c->pend_out = d_inMST;
+    if (opts) c->pend_opts = *opts;
+    else ecl_default_opts(&c->pend_opts);
+    c->pend_stream = stream ? (cudaStream_t)stream : c->stream;
+  }
+  return st;
+}
+
 extern "C" int ecl_mst_ctx_run_host(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* inMST,
                                     const mst_opts* opts, ecl_mst_stats* stats) {
   int st = check_graph_args(c, g, inMST);
@@ -686,6 +780,10 @@ extern "C" int ecl_mst_ctx_run_host(ecl_mst_ctx* c, const ecl_graph* g, uint8_t*
   if (m > 0)
     ECL_CUDA_TRY(cudaMemcpyAsync(inMST, c->d_inMST, (size_t)m, cudaMemcpyDeviceToHost, c->stream));
   if ((st = ecl_mst_ctx_sync(c))) return st;
+  if (c->resolved && m > 0) {  // the solve was repeated after a worklist overflow
+    ECL_CUDA_TRY(cudaMemcpyAsync(inMST, c->d_inMST, (size_t)m, cudaMemcpyDeviceToHost, c->stream));
+    ECL_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
   if (stats) {
     int64_t fe = 0;
     uint64_t fw = 0;
@@ -991,6 +1089,9 @@ extern "C" int ecl_batch_ctx_create(int device, int32_t max_graphs, int64_t max_
   if (max_graph_edges > c->cap || max_graph_nodes > c->cap) {
     if ((st = ecl_mst_ctx_create(device, max_graph_nodes, std::max<int64_t>(max_graph_edges, 1), &c->big)))
       return fail(st);
+    // the batch's solves are captured and replayed without a host check in
+    // between: lists that hold every entry of any input
+    if ((st = alloc_worklists(c->big, true))) return fail(st);
   }
   *out = c;
   return ECL_OK;

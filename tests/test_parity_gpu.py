@@ -336,3 +336,38 @@ def test_repeated_solve_is_captured_and_replayed(ctx):
             want, _, _ = O.oracle_mst(g.nindex, g.nlist, w, st["threshold"], st["filtered"])
             assert np.array_equal(out.cpu().numpy(), want), (kw, step)
             assert st["ms_total"] > 0 and st["status"] == 0
+
+
+def _forward_only(n, k, seed):
+    """Every undirected edge stored once, forward (nlist[j] > v): v -> v+1 .. v+k.
+    All m entries are one-direction entries, twice what a symmetric input has."""
+    v = np.repeat(np.arange(n - k, dtype=np.int64), k)
+    nb = v + np.tile(np.arange(1, k + 1), n - k)
+    nindex = np.zeros(n + 1, np.int32)
+    nindex[1:] = np.cumsum(np.bincount(v, minlength=n))
+    w = np.random.default_rng(seed).integers(1, 1 << 20, len(nb)).astype(np.int32)
+    return E.Graph(nindex, nb.astype(np.int32), w)
+
+
+@pytest.mark.parametrize("k", [3, 6])
+def test_one_direction_input_grows_the_worklists(k):
+    """Contexts size their worklists for symmetric input (edges/2 one-direction
+    entries plus slack). An input with more overflows them; the library grows
+    them and repeats the solve on each synchronising path: run_host, a device
+    solve with stats, and a device solve checked by ctx_sync."""
+    import torch
+    g = _forward_only(1 << 20, k, 5 + k)
+    t, f = E.heuristic_threshold(g)
+    want, w, _ = O.oracle_mst(g.nindex, g.nlist, g.eweight, t, f)
+    with E.Context(g.nodes, g.edges) as c:
+        got, st = c.run_host(g)
+        assert st["status"] == 0 and np.array_equal(got, want) and st["forest_weight"] == w
+    dev = torch.device("cuda:0")
+    ni, nl, ew = (torch.from_numpy(a).to(dev) for a in (g.nindex, g.nlist, g.eweight))
+    for stats in (True, False):
+        with E.Context(g.nodes, g.edges) as c:
+            out = torch.full((g.edges,), 7, dtype=torch.uint8, device=dev)
+            c.run_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(),
+                         stream=torch.cuda.current_stream().cuda_stream, stats=stats)
+            c.sync()
+            assert np.array_equal(out.cpu().numpy(), want), stats
