@@ -205,6 +205,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_small(BatchArgs b) {
   int4* wl0 = b.wl_pool + (size_t)blockIdx.x * 2 * b.cap_m;
   int4* wl1 = wl0 + b.cap_m;
   round_smem_clear(s);
+  seg_set_dense(s, 0);  // one CTA per graph: every round list is dense from 0
   __syncthreads();
   for (;;) {
     if (threadIdx.x == 0) {

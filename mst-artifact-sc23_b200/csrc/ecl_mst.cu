@@ -264,7 +264,8 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
     return fail(st);
   for (auto& e : c->ev)
     if ((st = cuda_status(cudaEventCreate(&e)))) return fail(st);
-  c->round_grid = coop_grid((const void*)k_rounds, kRoundThreads,c->sm_count);
+  // every CTA of a round pass writes one segment of the round's output list
+  c->round_grid = std::min(coop_grid((const void*)k_rounds, kRoundThreads, c->sm_count), kMaxRoundCtas);
   if ((st = prepare_scan_kernels())) return fail(st);
   if (c->round_grid <= 0) return fail(ECL_ERR_CUDA);
   *out = c;
@@ -879,7 +880,7 @@ int na_setup(int dev, NaDevice** out) {
     ECL_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     if (!coop) return ECL_ERR_UNSUPPORTED;
     ECL_CUDA_TRY(cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev));
-    d.round_grid = coop_grid((const void*)k_rounds, kRoundThreads,d.sm_count);
+    d.round_grid = std::min(coop_grid((const void*)k_rounds, kRoundThreads, d.sm_count), kMaxRoundCtas);
     int ps = prepare_scan_kernels();
     if (ps) return ps;
     if (d.round_grid <= 0) return ECL_ERR_CUDA;

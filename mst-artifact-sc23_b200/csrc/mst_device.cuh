@@ -716,8 +716,11 @@ __global__ void __launch_bounds__(kThreads) k_flatten(int* parent, int n, const 
 // every entry's parent read, min-slot guard read, atomicMin and reset on one
 // L2 address; these small direct-mapped tables absorb the repeats per CTA.
 struct RoundSmem {
-  ReserveSmem rs;
-  unsigned kept;             // entries the CTA kept in the current find/min pass (tile totals)
+  ReserveSmem rs;            // the batch kernel's CTA scans
+  unsigned cursor;           // entries this CTA kept so far in the current find/min pass
+  int seg_n;                 // segments of the list the passes read (1 = dense from seg_off[0])
+  unsigned seg_q[kMaxRoundCtas + 1];  // entries in the segments before b (seg_q[seg_n] = all)
+  unsigned seg_off[kMaxRoundCtas];    // first position of segment b
   int hot_rep[kHotSlots];    // hot representative -> CTA-local partial minimum
   u64 hot_key[kHotSlots];
   int reset_seen[kHotSlots]; // previous-round slots this CTA already cleared
@@ -730,7 +733,7 @@ __device__ __forceinline__ unsigned hot_slot(int r) { return ((unsigned)r * 0x9E
 __device__ __forceinline__ unsigned find_slot(int r) { return ((unsigned)r * 0x85EBCA6Bu) >> (32 - kFindLog); }
 
 __device__ __forceinline__ void round_smem_clear(RoundSmem& s) {
-  if (threadIdx.x == 0) s.kept = 0;
+  if (threadIdx.x == 0) s.cursor = 0;
   for (int i = threadIdx.x; i < kHotSlots; i += blockDim.x) {
     s.hot_rep[i] = -1;
     s.hot_key[i] = kNoEdge;
@@ -747,23 +750,99 @@ __device__ __forceinline__ unsigned pair_slot(u64 pk) {
   return (unsigned)((pk * 0x9E3779B97F4A7C15ull) >> (64 - kPairLog));
 }
 
-// The tile's worklist reservation, optionally fused with parallel-edge
-// elimination (`dedup`, opt-in through ECL_FLAG_DEDUP). Entries of one tile
-// that join the same two trees are parallel edges of the contracted graph;
-// only the one with the smallest (weight, j) key can be a forest edge (any
-// forest through a heavier one is heavier than the same forest through the
-// lightest), so the others may be dropped for good. Warp groups with equal
-// rep pairs reduce first; group minima meet in a per-tile shared table.
-// Measured on RMAT scale 22 the elimination costs more (a third CTA barrier
-// and the table per tile) than the smaller worklists save, so it is off by
-// default. keep[k] is narrowed to the survivors, and *pos receives the first
-// output slot of this thread's survivors (one global atomic per CTA tile).
-// Every thread of the CTA must call this.
+// ---- segmented round worklists
+// A find/min pass compacts its kept entries without any global reservation:
+// the CTA that runs tile share b of the pass (tiles b, b + stride, ...) owns
+// the output positions [region_b, region_b + share_b), where share_b counts
+// the logical input entries of its tiles, and its warps take positions from a
+// shared-memory cursor. The pass's output is therefore one dense segment per
+// CTA (seg_cnt[b] kept entries from region_b). The next passes address that
+// list by logical index through a prefix table of the segment counts, so a
+// pass needs neither a global atomic per tile nor a CTA barrier per tile.
+
+// The list read next is dense: entries [0, count) from position 0.
+__device__ __forceinline__ void seg_set_dense(RoundSmem& s, unsigned count) {
+  if (threadIdx.x == 0) {
+    s.seg_n = 1;
+    s.seg_off[0] = 0;
+    s.seg_q[0] = 0;
+    s.seg_q[1] = count;
+  }
+}
+
+// The list read next is the one the grid's find/min pass just wrote (`nseg`
+// segments, published in the control block before the grid barrier). One
+// warp builds the prefix table; the caller synchronises the CTA before use.
+__device__ __forceinline__ void seg_load(RoundSmem& s, const DevState* st, int nseg) {
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  const int per = (nseg + 31) >> 5;
+  const int b0 = lane * per;
+  unsigned sum = 0;
+  for (int k = 0; k < per; k++) {
+    const int b = b0 + k;
+    if (b < nseg) {
+      const unsigned c = __ldcg(&st->seg_cnt[b]);
+      s.seg_off[b] = __ldcg(&st->seg_off[b]);
+      s.seg_q[b] = sum;
+      sum += c;
+    }
+  }
+  unsigned incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const unsigned excl = incl - sum;
+  for (int k = 0; k < per; k++) {
+    const int b = b0 + k;
+    if (b < nseg) s.seg_q[b] += excl;
+  }
+  if (lane == 31) {
+    s.seg_q[nseg] = incl;
+    s.seg_n = nseg;
+  }
+}
+
+// Position of logical entry i of the list described by the prefix table.
+__device__ __forceinline__ unsigned seg_at(const RoundSmem& s, unsigned i) {
+  const int nseg = s.seg_n;
+  if (nseg == 1) return s.seg_off[0] + i;
+  int lo = 0, hi = nseg;  // largest b with seg_q[b] <= i (seg_q[nseg] > i)
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (s.seg_q[mid] <= i) lo = mid;
+    else hi = mid;
+  }
+  return s.seg_off[lo] + (i - s.seg_q[lo]);
+}
+
+// First output position of tile share `b` of a pass over W logical entries
+// in tiles of `tile`, shares strided by `stride`: the logical entries of the
+// tiles of all shares before b (the last tile may be partial).
+__device__ __forceinline__ unsigned share_region(unsigned W, unsigned tile, unsigned b, unsigned stride) {
+  const unsigned ntiles = (W + tile - 1) / tile;
+  const unsigned q = ntiles / stride, rr = ntiles % stride;
+  const unsigned long long full = (unsigned long long)tile * ((unsigned long long)q * b + min(b, rr));
+  const unsigned last_owner = ntiles ? (ntiles - 1) % stride : 0u;
+  const unsigned short_by = (unsigned)((unsigned long long)ntiles * tile - W);
+  return (unsigned)(full - (ntiles && b > last_owner ? short_by : 0u));
+}
+
+// Parallel-edge elimination within a tile (opt-in through ECL_FLAG_DEDUP).
+// Entries of one tile that join the same two trees are parallel edges of the
+// contracted graph; only the one with the smallest (weight, j) key can be a
+// forest edge (any forest through a heavier one is heavier than the same
+// forest through the lightest), so the others may be dropped for good. Warp
+// groups with equal rep pairs reduce first; group minima meet in a per-tile
+// shared table. Measured on RMAT scale 22 the elimination costs more (two CTA
+// barriers and the table per tile) than the smaller worklists save, so it is
+// off by default. keep[k] is narrowed to the survivors. Every thread of the
+// CTA must call this (it synchronises the CTA).
 template <int E>
-__device__ __forceinline__ void drop_parallel_reserve(const int4 (&e)[E], bool (&keep)[E],
-                                                      unsigned* ctr, RoundSmem& s, unsigned* pos,
-                                                      bool dedup) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+__device__ __forceinline__ void drop_parallel(const int4 (&e)[E], bool (&keep)[E], RoundSmem& s) {
+  const int lane = threadIdx.x & 31;
   u64 pk[E], gmin[E];
 #pragma unroll
   for (int k = 0; k < E; k++) {
@@ -771,7 +850,6 @@ __device__ __forceinline__ void drop_parallel_reserve(const int4 (&e)[E], bool (
     pk[k] = keep[k] ? (((u64)lo << 32) | hi) : (0xFFFFFFFF00000000ull | (threadIdx.x * E + k));
     const u64 key = edge_key(e[k].z, e[k].w);
     gmin[k] = key;
-    if (!dedup) continue;  // uniform across the CTA
     const unsigned g = __match_any_sync(0xffffffffu, pk[k]);
     if (!keep[k]) continue;
     if (g & (g - 1)) {
@@ -790,48 +868,52 @@ __device__ __forceinline__ void drop_parallel_reserve(const int4 (&e)[E], bool (
       if (t == pk[k] && ((volatile u64*)s.pair_min)[slot] > gmin[k]) atomicMin(&s.pair_min[slot], gmin[k]);
     }
   }
-  if (dedup) __syncthreads();  // S1: the tile's pair table is complete
-  unsigned cnt = 0;
+  __syncthreads();  // the tile's pair table is complete
 #pragma unroll
   for (int k = 0; k < E; k++) {
-    if (dedup && keep[k]) {
+    if (keep[k]) {
       const unsigned slot = pair_slot(pk[k]);
       const u64 key = edge_key(e[k].z, e[k].w);
       const u64 best = s.pair_tag[slot] == pk[k] ? s.pair_min[slot] : gmin[k];
       keep[k] = key == best;
     }
-    cnt += keep[k];
   }
-  unsigned incl = cnt;
+  __syncthreads();  // every check done before the table is cleared
+  for (int i = threadIdx.x; i < kPairSlots; i += blockDim.x) {
+    s.pair_tag[i] = kNoPair;
+    s.pair_min[i] = kNoEdge;
+  }
+}
+
+// Output positions for this thread's kept entries: one shared-memory atomic
+// per warp on the CTA's cursor, no barrier. Returns the position of the
+// thread's first kept entry (the rest follow) inside the CTA's segment that
+// starts at `region`. Every lane of the warp must call this.
+template <int E>
+__device__ __forceinline__ unsigned warp_reserve(const bool (&keep)[E], RoundSmem& s, unsigned region) {
+  const int lane = threadIdx.x & 31;
+  unsigned cnt = 0;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += t;
-  }
-  if (lane == 31) s.rs.warp_off[warp][0] = incl;
-  __syncthreads();  // S2: every check done, warp totals written
-  if (dedup)
-    for (int i = threadIdx.x; i < kPairSlots; i += blockDim.x) {
-      s.pair_tag[i] = kNoPair;
-      s.pair_min[i] = kNoEdge;
-    }
-  if (warp == 0) {
-    const int nw = blockDim.x >> 5;
-    const unsigned w0 = lane < nw ? s.rs.warp_off[lane][0] : 0u;
-    unsigned x0 = w0;
+  for (int k = 0; k < E; k++) cnt += keep[k];
+  unsigned excl, total;
+  if (E == 1) {
+    const unsigned mask = __ballot_sync(0xffffffffu, cnt != 0);
+    excl = __popc(mask & ((1u << lane) - 1u));
+    total = __popc(mask);
+  } else {
+    unsigned incl = cnt;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const unsigned t = __shfl_up_sync(0xffffffffu, x0, o);
-      if (lane >= o) x0 += t;
+      const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
     }
-    if (lane < nw) s.rs.warp_off[lane][0] = x0 - w0;
-    if (lane == 31) {
-      s.rs.base[0] = x0 ? atomicAdd(ctr, x0) : 0u;
-      s.kept += x0;  // the tile's survivors (one thread updates it)
-    }
+    excl = incl - cnt;
+    total = __shfl_sync(0xffffffffu, incl, 31);
   }
-  __syncthreads();  // S3: offsets and the tile's base are published
-  *pos = s.rs.base[0] + s.rs.warp_off[warp][0] + (incl - cnt);
+  unsigned base = 0;
+  if (lane == 0 && total) base = atomicAdd(&s.cursor, total);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  return region + base + excl;
 }
 
 // Roots of the 2*kEPT endpoints a thread holds, all walks advanced in lock
@@ -991,7 +1073,10 @@ __device__ __forceinline__ void offer_mins(const int (&rep)[N], const u64 (&key)
 // each input entry clears its endpoints' slots in the previous round's min
 // array, resolves its endpoints to reps, and if they differ is compacted into
 // `out` with the reps (implicit path compression, :218-219) and offers its
-// key to both reps' min slots.
+// key to both reps' min slots. The input is the list the prefix table in `s`
+// describes (W logical entries); the kept entries go to this CTA's segment of
+// `out` (share `start` of `stride`), whose size is left in s.cursor and
+// added to *out_ctr and *kept_ctr.
 //
 // `fresh` marks the first round of a phase: its entries come straight from
 // the scan, so both endpoints are roots (parent[v] = v before the light
@@ -1005,6 +1090,8 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
   constexpr int N = 2 * kEPT;
   const unsigned tile = blockDim.x * kEPT;
   const unsigned ntiles = (W + tile - 1) / tile;
+  const unsigned region = share_region(W, tile, start, stride);
+  const bool dedup = (a.abl & kDedup) != 0;
   unsigned long long atomics = 0;
   if (reset == kResetDense)  // every slot of the previous round's array, coalesced
     for (unsigned i = start * blockDim.x + threadIdx.x; i < (unsigned)a.nodes; i += stride * blockDim.x)
@@ -1016,7 +1103,7 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
     for (int k = 0; k < kEPT; k++) {
       const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
       in_range[k] = idx < W;
-      e[k] = in_range[k] ? __ldcg(in + idx) : make_int4(0, 0, 0, 0);
+      e[k] = in_range[k] ? __ldcg(in + seg_at(s, idx)) : make_int4(0, 0, 0, 0);
       if (e[k].x < 0) in_range[k] = false;  // null entry (unused scan slot)
     }
     int v[N];
@@ -1043,8 +1130,8 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
         e[k].x = v[2 * k];
         e[k].y = v[2 * k + 1];
       }
-      unsigned pos;
-      drop_parallel_reserve<kEPT>(e, keep, out_ctr, s, &pos, (a.abl & kDedup) != 0);
+      if (dedup) drop_parallel<kEPT>(e, keep, s);  // uniform across the CTA
+      unsigned pos = warp_reserve<kEPT>(keep, s, region);
 #pragma unroll
       for (int k = 0; k < kEPT; k++) {
         if (keep[k]) {
@@ -1064,7 +1151,10 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
     offer_mins<N>(v, key, kv, mcur, s, atomics, !(a.abl & kAblNoCoop), !(a.abl & kAblNoGuards));
   }
   __syncthreads();
-  if (threadIdx.x == 0 && s.kept) atomicAdd(kept_ctr, s.kept);
+  if (threadIdx.x == 0 && s.cursor) {
+    atomicAdd(out_ctr, s.cursor);
+    atomicAdd(kept_ctr, s.cursor);
+  }
   // flush the CTA's partial minima of hot representatives
   for (int i = threadIdx.x; i < kHotSlots; i += blockDim.x) {
     const int r = s.hot_rep[i];
@@ -1089,7 +1179,8 @@ __device__ __forceinline__ void hot_refresh(const u64* mcur, RoundSmem& s) {
 }
 
 // kernel2 (ECL_MST.cu:229-240): an entry whose key is the minimum of either
-// endpoint's slot is a forest edge: union the trees and mark inMST[j].
+// endpoint's slot is a forest edge: union the trees and mark inMST[j]. The
+// list is the one the prefix table in `s` describes (W logical entries).
 __device__ __forceinline__ void round_mark(const RoundArgs& a, const int4* wl, unsigned W,
                                            const u64* mcur, unsigned start, unsigned stride,
                                            const RoundSmem& s) {
@@ -1102,7 +1193,7 @@ __device__ __forceinline__ void round_mark(const RoundArgs& a, const int4* wl, u
     for (int k = 0; k < kEPT; k++) {
       const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
       in_range[k] = idx < W;
-      e[k] = in_range[k] ? __ldcg(wl + idx) : make_int4(0, 0, 0, 0);
+      e[k] = in_range[k] ? __ldcg(wl + seg_at(s, idx)) : make_int4(0, 0, 0, 0);
       if (e[k].x < 0) in_range[k] = false;  // null entry (unused scan slot)
     }
     u64 mx[kEPT], my[kEPT];
@@ -1134,6 +1225,7 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
   // Only bits no CTA of this kernel can set, so every CTA takes the same exit.
   if (ld_volatile(&st->error) & (kErrFormat | kErrTimeout)) return;
   round_smem_clear(s);
+  seg_set_dense(s, 0);  // round 0 reads the scan's list as it is
   __syncthreads();
   bool tail = false;
   int r = 0;
@@ -1168,12 +1260,22 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
       st->wl_count[ph][1] = W;
       st->wl_kept[ph][1] = st->scan_kept[ph];
     }
+    if (!fresh && !tail && threadIdx.x == 0) {  // this CTA's segment of the output list
+      st->seg_cnt[blockIdx.x] = s.cursor;
+      st->seg_off[blockIdx.x] = share_region(W, blockDim.x * kEPT, blockIdx.x, gridDim.x);
+    }
     if (tail) __syncthreads();
     else if (!grid_barrier(st, kBarrierTimeoutNs)) return;
     if (stamp) st->t_round[ph][2 * r] = globaltimer_ns();
     const unsigned W2 = min(ld_volatile(&st->wl_count[ph][r + 1]), a.wl_cap);
     r++;
     if (W2 == 0) break;
+    // the list the mark pass and the next round read: the scan's list (round
+    // 0), the tail CTA's single segment, or the grid's per-CTA segments
+    if (!fresh) {
+      if (tail) seg_set_dense(s, s.cursor);
+      else seg_load(s, st, (int)gridDim.x);
+    }
     hot_refresh(mcur, s);
     round_mark(a, fresh ? in : out, W2, mcur, start, stride, s);
     __syncthreads();

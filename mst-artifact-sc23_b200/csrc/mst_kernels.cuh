@@ -20,6 +20,10 @@ enum : unsigned {
   kErrRounds = 8u     // more Boruvka rounds than ECL_MAX_ROUNDS
 };
 
+// Most CTAs a round-kernel launch may have: each CTA of a find/min pass
+// writes its kept entries as one segment of the round's output list.
+constexpr int kMaxRoundCtas = 1024;
+
 constexpr int kChunkLog = 7;  // long rows are scanned in aligned 128-entry chunks
 constexpr int kChunk = 1 << kChunkLog;
 constexpr u64 kNoEdge = ~0ull;
@@ -45,6 +49,11 @@ struct DevState {
   u64 t_round[2][2 * ECL_MAX_ROUNDS];
   unsigned scan_kept[2];  // entries each scan kept (wl_count[p][0] also counts padding)
   unsigned wl_kept[2][ECL_MAX_ROUNDS + 1];  // [phase][r + 1] = entries round r kept (no padding)
+  // The last find/min pass's output list, one segment per CTA: CTA b wrote
+  // seg_cnt[b] entries from position seg_off[b] (written before the grid
+  // barrier that ends the pass, read after it).
+  unsigned seg_cnt[kMaxRoundCtas];
+  unsigned seg_off[kMaxRoundCtas];
 };
 
 __device__ __forceinline__ u64 globaltimer_ns() {
