@@ -564,10 +564,18 @@ def main():
     ablation = None
     if not args.profile and not args.no_ablation:
         E_ = E
+        nag_nw = E_.FLAG_NO_GUARDS | E_.FLAG_NO_WARP_COOP
+        nipc = nag_nw | E_.FLAG_NO_IMPLICIT_COMPRESSION
         series = [("base", 0, E_.THRESH_HEURISTIC),
                   ("NAG", E_.FLAG_NO_GUARDS, E_.THRESH_HEURISTIC),
-                  ("NAG_NW", E_.FLAG_NO_GUARDS | E_.FLAG_NO_WARP_COOP, E_.THRESH_HEURISTIC),
-                  ("NAG_NW_NF", E_.FLAG_NO_GUARDS | E_.FLAG_NO_WARP_COOP, E_.THRESH_NONE),
+                  ("NAG_NW", nag_nw, E_.THRESH_HEURISTIC),
+                  ("NAG_NW_NF", nag_nw, E_.THRESH_NONE),
+                  # the reference's later steps (NOD is not reproduced: it changes inMST)
+                  ("NAG_NW_NF_NIPC", nipc, E_.THRESH_NONE),
+                  ("NAG_NW_NF_NIPC_NT", nipc | E_.FLAG_NO_TUPLES, E_.THRESH_NONE),
+                  ("NAG_NW_NF_NIPC_NT_NDD", nipc | E_.FLAG_NO_TUPLES | E_.FLAG_NO_DATA_DRIVEN, E_.THRESH_NONE),
+                  ("NAG_NW_NF_NIPC_NT_NDD_NEB", nipc | E_.FLAG_NO_TUPLES | E_.FLAG_NO_DATA_DRIVEN
+                   | E_.FLAG_NO_EDGE_BASED, E_.THRESH_NONE),
                   ("with_dedup", E_.FLAG_DEDUP, E_.THRESH_HEURISTIC),
                   ("no_find_cache", E_.FLAG_NO_FIND_CACHE, E_.THRESH_HEURISTIC),
                   ("no_small_tail", E_.FLAG_NO_SMALL_TAIL, E_.THRESH_HEURISTIC)]
@@ -575,7 +583,8 @@ def main():
         for name, flags, tmode in series:
             o = E_.make_opts(mode=tmode, degree_split=args.split, flags=flags)
             ms = []
-            for i in range(2 + 5):
+            slow = "NIPC" in name  # the later steps are slow: fewer repeats
+            for i in range(2 + (2 if slow else 5)):
                 flush.max()
                 st_a = ctx.run_device(g.nodes, g.edges, d_ni.data_ptr(), d_nl.data_ptr(), d_ew.data_ptr(),
                                       d_out.data_ptr(), opts=o, stream=stream.cuda_stream, stats=True)

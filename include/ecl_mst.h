@@ -205,7 +205,30 @@ enum {
    * the first repeat and replayed as one launch after that; a replayed
    * solve's stats carry ms_total only. NO_GRAPH keeps direct launches (and
    * the per-phase timings). */
-  ECL_FLAG_NO_GRAPH = 1 << 7
+  ECL_FLAG_NO_GRAPH = 1 << 7,
+  /* The reference's later deoptimization steps (Deoptimizations/, the
+   * ablation of generate_deoptimize_tables.py:6-14), restated so that the
+   * forest is unchanged: one direction is kept (the reference's
+   * NoOneDirection step marks the reverse entry instead and is not
+   * reproduced). Single-graph contexts only; the batched and the
+   * allocation-free entry points return ECL_ERR_UNSUPPORTED for them. */
+  ECL_FLAG_NO_IMPLICIT_COMPRESSION = 1 << 8, /* compacted entries keep their
+                                      endpoints; finds split paths from the
+                                      first step; the mark pass finds again
+                                      (..._NoImplicitPathCompression.cu:121-133,
+                                      193-216)                                */
+  ECL_FLAG_NO_TUPLES = 1 << 9,     /* worklists hold CSR indices; endpoints and
+                                      weights are gathered every round through
+                                      a per-entry vertex list (..._NoTuples.cu;
+                                      implies NO_IMPLICIT_COMPRESSION; the
+                                      context allocates the list on first use) */
+  ECL_FLAG_NO_DATA_DRIVEN = 1 << 10, /* topology-driven: every round reads the
+                                      phase's whole list, nothing is compacted
+                                      (..._NoDataDriven.cu:166-180, 263-270;
+                                      implies NO_IMPLICIT_COMPRESSION)         */
+  ECL_FLAG_NO_EDGE_BASED = 1 << 11 /* vertex-centric rounds over the CSR, one
+                                      thread per vertex, no worklists
+                                      (..._NoEdgeBased.cu:152-195)             */
 };
 
 typedef struct mst_opts {

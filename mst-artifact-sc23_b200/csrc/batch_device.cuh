@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_small(BatchArgs b) {
     }
     __syncthreads();
     const int thr = sh_thr, filtered = sh_filtered;
-    RoundArgs ra;
+    RoundArgs ra{};
     ra.phase = 0;
     ra.nodes = n;
     ra.wl0 = wl0;

@@ -61,6 +61,8 @@ struct ecl_mst_ctx {
   mst_opts pend_opts = {};
   cudaStream_t pend_stream = nullptr;
   bool resolved = false;  // the last ecl_mst_ctx_sync repeated the solve
+  int* slist = nullptr;    // ECL_FLAG_NO_TUPLES: vertex of every CSR entry (allocated on first use)
+  int vertex_grid = 0;     // ECL_FLAG_NO_EDGE_BASED: cooperative grid of the vertex-centric rounds
   int* first_v = nullptr;  // tile -> vertex table of the edge-balanced scans
   int first_v_cap = 0;
   DevState* st = nullptr;
@@ -187,8 +189,14 @@ int enqueue_prep(const PrepArgs& pa, int sm_count, cudaStream_t s, const cudaAcc
 // Round-kernel ablation bits from the option flags.
 unsigned round_ablation(int flags) {
   return ((flags & ECL_FLAG_NO_GUARDS) ? kAblNoGuards : 0u) | ((flags & ECL_FLAG_NO_WARP_COOP) ? kAblNoCoop : 0u) |
-         ((flags & ECL_FLAG_DEDUP) ? kDedup : 0u) | ((flags & ECL_FLAG_NO_FIND_CACHE) ? kAblNoFindCache : 0u);
+         ((flags & ECL_FLAG_DEDUP) ? kDedup : 0u) | ((flags & ECL_FLAG_NO_FIND_CACHE) ? kAblNoFindCache : 0u) |
+         ((flags & ECL_FLAG_NO_IMPLICIT_COMPRESSION) ? kAblNoIPC : 0u) |
+         ((flags & ECL_FLAG_NO_TUPLES) ? kAblNoTuples : 0u) | ((flags & ECL_FLAG_NO_DATA_DRIVEN) ? kAblNoDD : 0u);
 }
+
+// The reference's later ablation steps, which only the single-graph engine runs.
+constexpr int kDeoptFlags = ECL_FLAG_NO_IMPLICIT_COMPRESSION | ECL_FLAG_NO_TUPLES | ECL_FLAG_NO_DATA_DRIVEN |
+                            ECL_FLAG_NO_EDGE_BASED;
 
 }  // namespace
 
@@ -266,8 +274,9 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
     if ((st = cuda_status(cudaEventCreate(&e)))) return fail(st);
   // every CTA of a round pass writes one segment of the round's output list
   c->round_grid = std::min(coop_grid((const void*)k_rounds, kRoundThreads, c->sm_count), kMaxRoundCtas);
+  c->vertex_grid = coop_grid((const void*)k_rounds_vertex, kRoundThreads, c->sm_count);
   if ((st = prepare_scan_kernels())) return fail(st);
-  if (c->round_grid <= 0) return fail(ECL_ERR_CUDA);
+  if (c->round_grid <= 0 || c->vertex_grid <= 0) return fail(ECL_ERR_CUDA);
   *out = c;
   return ECL_OK;
 }
@@ -284,6 +293,7 @@ extern "C" void ecl_mst_ctx_destroy(ecl_mst_ctx* c) {
   cudaFree(c->wl[0]);
   cudaFree(c->wl[1]);
   cudaFree(c->first_v);
+  cudaFree(c->slist);
   cudaFree(c->ml_params);
   cudaFree(c->ml_feat);
   cudaFree(c->ml_acc);
@@ -455,7 +465,13 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   int st;
   if ((st = enqueue_prep(pa, c->sm_count, s, win_all))) return st;
   if (join) ECL_CUDA_TRY(cudaStreamWaitEvent(s, join, 0));
-  ScanArgs sa;
+  const bool no_tuples = (o->flags & (ECL_FLAG_NO_TUPLES | ECL_FLAG_NO_EDGE_BASED)) == ECL_FLAG_NO_TUPLES;
+  if (no_tuples) {  // the vertex of every entry, for the gathers of the rounds
+    const int sgrid = (int)std::min<int64_t>(((int64_t)m + kThreads - 1) / kThreads, (int64_t)c->sm_count * 16);
+    k_slist<<<std::max(sgrid, 1), kThreads, 0, s>>>(g->nindex, c->first_v, c->slist, m, c->st);
+    ECL_CUDA_TRY(cudaGetLastError());
+  }
+  ScanArgs sa{};
   sa.nodes = n;
   sa.edges = m;
   sa.nindex = g->nindex;
@@ -474,7 +490,8 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   sa.zero_vec = (((uintptr_t)d_inMST) & 15) == 0;
   sa.st = c->st;
   sa.sm_count = c->sm_count;
-  RoundArgs ra;
+  sa.ids = no_tuples ? 1 : 0;
+  RoundArgs ra{};
   ra.nodes = n;
   ra.wl0 = c->wl[0];
   ra.wl1 = c->wl[1];
@@ -488,7 +505,32 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   if (o->flags & ECL_FLAG_NO_SMALL_TAIL) ra.small_tail = 0;
   ra.count_atomics = (o->flags & ECL_FLAG_STATS) ? 1 : 0;
   ra.abl = round_ablation(o->flags);
+  ra.nlist = g->nlist;
+  ra.eweight = g->eweight;
+  ra.slist = c->slist;
+  // entries that keep their endpoints clear the whole previous min array
+  // each round, which one CTA of a small tail would do alone
+  if (ra.abl & kAblKeepEnds) ra.small_tail = 0;
   const int rgrid = std::max(1, std::min(c->round_grid, (m / 2 + kRoundThreads - 1) / kRoundThreads + 1));
+  if (o->flags & ECL_FLAG_NO_EDGE_BASED) {
+    // vertex-centric rounds straight over the CSR: no scans, no worklists
+    if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[5], s));
+    ECL_CUDA_TRY(cudaMemsetAsync(d_inMST, 0, (size_t)m, s));
+    if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+    ra.phase = 0;
+    if ((st = launch_ex(k_rounds_vertex, c->vertex_grid, kRoundThreads, 0, s, true, nullptr, ra, g->nindex)))
+      return st;
+    if (timed) {
+      ECL_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+      ECL_CUDA_TRY(cudaEventRecord(c->ev[6], s));
+      ECL_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+    }
+    ra.phase = 1;
+    if ((st = launch_ex(k_rounds_vertex, c->vertex_grid, kRoundThreads, 0, s, true, nullptr, ra, g->nindex)))
+      return st;
+    if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[4], s));
+    return ECL_OK;
+  }
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[5], s));
   if ((st = launch_scans<kLight>(device_split, split, sa, s, nullptr))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[1], s));
@@ -629,6 +671,8 @@ int run_device_once(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d_inMST, const 
   if (o.threshold_mode == ECL_THRESH_LEARNED && (g->edges < kLearnedMinEdges || !ecl_learned_has_weights()))
     o.threshold_mode = ECL_THRESH_HEURISTIC;
   const bool timed = stats != nullptr;
+  if ((o.flags & ECL_FLAG_NO_TUPLES) && !c->slist)  // the ablation's per-entry vertex list, once
+    ECL_CUDA_TRY(cudaMalloc(&c->slist, (size_t)std::max<int64_t>(c->max_edges, 1) * sizeof(int)));
   if (o.flags & ECL_FLAG_L2_PERSIST) {
     // Persisting set-aside for this process's context, sized for the solve's
     // slot arrays (20n bytes) up to the device maximum; set before any
@@ -907,6 +951,7 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   // not hold; it takes the reference heuristic, as ecl_mst_run_device does
   // below its learned-schedule cut-off.
   if (o.threshold_mode == ECL_THRESH_LEARNED) o.threshold_mode = ECL_THRESH_HEURISTIC;
+  if (o.flags & kDeoptFlags) return ECL_ERR_UNSUPPORTED;  // single-graph contexts only
   if (g->edges == 0) return ECL_OK;
   int dev = 0;
   ECL_CUDA_TRY(cudaGetDevice(&dev));
@@ -943,7 +988,7 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   pa.quantile = o.quantile;
   pa.st = dst;
   if ((st = enqueue_prep(pa, d->sm_count, s))) return st;
-  ScanArgs sa;
+  ScanArgs sa{};
   sa.nodes = n;
   sa.edges = m;
   sa.nindex = g->nindex;
@@ -961,7 +1006,7 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   sa.zero_vec = (((uintptr_t)d_inMST) & 15) == 0;
   sa.st = dst;
   sa.sm_count = d->sm_count;
-  RoundArgs ra;
+  RoundArgs ra{};
   ra.nodes = n;
   ra.wl0 = wl0;
   ra.wl1 = wl1;
@@ -1273,6 +1318,7 @@ extern "C" int ecl_mst_run_batch_device(ecl_batch_ctx* c, const ecl_batch* b, ui
   else ecl_default_opts(&o);
   int st = check_opts(&o);
   if (st) return st;
+  if (o.flags & kDeoptFlags) return ECL_ERR_UNSUPPORTED;  // single-graph contexts only
   ECL_CUDA_TRY(cudaSetDevice(c->device));
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
   if ((st = batch_enqueue(c, b, d_inMST, &o, s, stats != nullptr, stats))) return st;

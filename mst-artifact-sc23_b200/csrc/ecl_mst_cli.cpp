@@ -9,10 +9,14 @@
 //
 // An optional third argument names a deoptimized variant the way the
 // reference's ablation binaries are named (Deoptimizations/
-// run_all_ECL-MST_deopts.sh): "NAG", "NAG_NW", "NAG_NW_NF" switch off the
-// atomic guards, the warp cooperation and the filter of this engine (the
-// forest is unchanged). The reference's later steps (NIPC, NOD, NT, NDD,
-// NEB) remove structure this engine is built on and are not reproduced.
+// run_all_ECL-MST_deopts.sh, generate_deoptimize_tables.py:6-14): the parts
+// NAG, NW, NF, NIPC, NT, NDD and NEB switch off the atomic guards, the warp
+// cooperation, the filter, implicit path compression, tuples, data-driven
+// worklists and edge-based kernels (mst_opts flags; the forest is
+// unchanged). NOD (both directions) would mark the reverse entry and change
+// inMST, so it is not reproduced: the part is accepted so that the
+// reference's variant names still run, and a note on stderr says it was
+// left out.
 //
 // ecl_mst --to-pbbs|--to-mtx <graph.egr> <out> converts a graph for the other
 // MST codes of the artifact, as PBBS_CPU/inputs/ecl2pbbs_genweights.cpp and
@@ -36,6 +40,12 @@ static bool variant_opts(const char* name, mst_opts* o) {
     if (part == "NAG") o->flags |= ECL_FLAG_NO_GUARDS;
     else if (part == "NW") o->flags |= ECL_FLAG_NO_WARP_COOP;
     else if (part == "NF") o->threshold_mode = ECL_THRESH_NONE;
+    else if (part == "NIPC") o->flags |= ECL_FLAG_NO_IMPLICIT_COMPRESSION;
+    else if (part == "NT") o->flags |= ECL_FLAG_NO_TUPLES;
+    else if (part == "NDD") o->flags |= ECL_FLAG_NO_DATA_DRIVEN;
+    else if (part == "NEB") o->flags |= ECL_FLAG_NO_EDGE_BASED;
+    else if (part == "NOD")
+      fprintf(stderr, "note: variant part NOD is not reproduced (it would mark the reverse entry); left out\n");
     else if (part != "base") return false;
     if (end == std::string::npos) break;
     pos = end + 1;
@@ -65,7 +75,8 @@ int main(int argc, char* argv[]) {
   if (argc == 4 && (strcmp(argv[1], "--to-pbbs") == 0 || strcmp(argv[1], "--to-mtx") == 0))
     return convert(argv[1], argv[2], argv[3]);
   if (argc < 2 || argc > 4 || argv[1][0] == '-') {
-    printf("USAGE: %s input_graph [runs] [variant: base | NAG | NAG_NW | NAG_NW_NF]\n"
+    printf("USAGE: %s input_graph [runs] [variant: base | NAG | NAG_NW | NAG_NW_NF | NAG_NW_NF_NIPC\n"
+           "         | NAG_NW_NF_NIPC_NOD_NT | NAG_NW_NF_NIPC_NOD_NT_NDD | NAG_NW_NF_NIPC_NOD_NT_NDD_NEB]\n"
            "       %s --to-pbbs | --to-mtx input_graph output_file\n", argv[0], argv[0]);
     return 1;
   }

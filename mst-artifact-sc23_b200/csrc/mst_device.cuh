@@ -100,6 +100,7 @@ struct ScanArgs {
   int sm_count;  // host side: sizes the persistent scan launch
   unsigned wl_slack;  // host side: wl_cap minus the most entries a scan can keep
   unsigned chunk;     // worklist slots a warp reserves at once (set at launch)
+  int ids;            // 1 = append CSR indices (int) instead of tuples (kAblNoTuples)
   DevState* st;
 };
 
@@ -117,6 +118,10 @@ struct RoundArgs {
   unsigned small_tail;
   int count_atomics;
   unsigned abl;  // kAbl* bits: techniques switched off to measure what they buy
+  // kAblNoTuples: the CSR and the vertex of every entry
+  const int* nlist;
+  const int* eweight;
+  const int* slist;
 };
 
 // Ablation switches of the round kernel (mst_opts flags ECL_FLAG_NO_*).
@@ -125,7 +130,20 @@ enum : unsigned {
   kAblNoCoop = 2u,       // no warp reduction or CTA table for shared reps
   kDedup = 4u,           // parallel-edge elimination on (opt-in: measured slower on RMAT)
   kAblNoFindCache = 8u,  // no per-CTA root cache in the finds
+  // The reference's later deoptimization steps, restated so that the forest
+  // stays the reference's (one direction is kept):
+  kAblNoIPC = 16u,     // NoImplicitPathCompression: compacted entries keep their
+                       // endpoints, finds split paths from the first step and
+                       // the mark pass finds again
+                       // (ECL_MST_..._NoImplicitPathCompression.cu:121-133, 193-216)
+  kAblNoTuples = 32u,  // NoTuples: worklists hold CSR indices; endpoints and
+                       // weight are gathered every round (..._NoTuples.cu)
+  kAblNoDD = 64u,      // NoDataDriven: every round reads the phase's whole list
+                       // and nothing is compacted; the rounds end when no entry
+                       // joins two trees (..._NoDataDriven.cu:166-180, 263-270)
 };
+// Switches under which worklist entries keep their endpoints (no rewrite to reps)
+constexpr unsigned kAblKeepEnds = kAblNoIPC | kAblNoTuples | kAblNoDD;
 
 // ------------------------------------------------------------------ prep
 // Threshold rule, by mode (run by one CTA). HEURISTIC restates main's rule
@@ -664,8 +682,9 @@ __global__ void __launch_bounds__(kScanThreads, ScanCfg<EPT>::kMinBlocks) k_scan
       for (int q = 0; q < EPT; q++) {
         if (!(cand & (1u << q))) continue;
         const unsigned slot = p < avail ? wpos + p : fresh + (p - avail);
-        if (slot < a.wl_cap) a.wl[slot] = make_int4(vtx[q], nrep[q], w[q], (int)(jl + q));
-        else atomicOr(&st->error, kErrOverflow);
+        if (slot >= a.wl_cap) atomicOr(&st->error, kErrOverflow);
+        else if (a.ids) reinterpret_cast<int*>(a.wl)[slot] = (int)(jl + q);
+        else a.wl[slot] = make_int4(vtx[q], nrep[q], w[q], (int)(jl + q));
         p++;
       }
       if (total > avail) {
@@ -679,7 +698,10 @@ __global__ void __launch_bounds__(kScanThreads, ScanCfg<EPT>::kMinBlocks) k_scan
   }
   if (idmax >= (unsigned)n) atomicOr(&st->error, kErrFormat);  // a neighbour id outside [0, n)
   for (unsigned p = wpos + lane; p < wend; p += 32)  // null entries in the unused slots
-    if (p < a.wl_cap) a.wl[p] = make_int4(-1, -1, 0, 0);
+    if (p < a.wl_cap) {
+      if (a.ids) reinterpret_cast<int*>(a.wl)[p] = -1;
+      else a.wl[p] = make_int4(-1, -1, 0, 0);
+    }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
   if (lane == 0 && kept) atomicAdd(&st->scan_kept[KIND], kept);
@@ -935,7 +957,8 @@ __device__ __forceinline__ int find_cached(const RoundSmem& s, int x) {
 
 template <int N>
 __device__ __forceinline__ void multi_find(int (&v)[N], const bool (&valid)[N], int* parent,
-                                           RoundSmem& s, bool use_cache = true) {
+                                           RoundSmem& s, bool use_cache = true,
+                                           int split_after = kSplitAfter) {
   int par[N], orig[N], first[N];  // first: the start vertex's parent
   unsigned miss = 0;
 #pragma unroll
@@ -972,7 +995,7 @@ __device__ __forceinline__ void multi_find(int (&v)[N], const bool (&valid)[N], 
 #pragma unroll
     for (int i = 0; i < N; i++) {
       if (par[i] != v[i]) {
-        if (step >= kSplitAfter && gp[i] != par[i]) __stcg(parent + v[i], gp[i]);
+        if (step >= split_after && gp[i] != par[i]) __stcg(parent + v[i], gp[i]);
         v[i] = par[i];
         par[i] = gp[i];
       }
@@ -1069,6 +1092,23 @@ __device__ __forceinline__ void offer_mins(const int (&rep)[N], const u64 (&key)
   }
 }
 
+// Worklist entry at position `pos`: a tuple {rep a, rep b, w, j}, or under
+// kAblNoTuples a CSR index whose endpoints and weight are gathered (x = -1
+// marks a null entry either way).
+__device__ __forceinline__ int4 load_entry(const RoundArgs& a, const int4* list, unsigned pos) {
+  if (a.abl & kAblNoTuples) {
+    const int j = __ldcg(reinterpret_cast<const int*>(list) + pos);
+    if (j < 0) return make_int4(-1, -1, 0, 0);
+    return make_int4(__ldg(a.slist + j), __ldg(a.nlist + j), __ldg(a.eweight + j), j);
+  }
+  return __ldcg(list + pos);
+}
+
+__device__ __forceinline__ void store_entry(const RoundArgs& a, int4* list, unsigned pos, const int4& e) {
+  if (a.abl & kAblNoTuples) reinterpret_cast<int*>(list)[pos] = e.w;
+  else list[pos] = e;
+}
+
 // kernel1 (ECL_MST.cu:210-226) plus kernel3 of the previous round (:243-251):
 // each input entry clears its endpoints' slots in the previous round's min
 // array, resolves its endpoints to reps, and if they differ is compacted into
@@ -1092,6 +1132,8 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
   const unsigned ntiles = (W + tile - 1) / tile;
   const unsigned region = share_region(W, tile, start, stride);
   const bool dedup = (a.abl & kDedup) != 0;
+  const bool keep_ends = (a.abl & kAblKeepEnds) != 0;  // entries are not rewritten to reps
+  const bool count_only = (a.abl & kAblNoDD) != 0;     // nothing is compacted
   unsigned long long atomics = 0;
   if (reset == kResetDense)  // every slot of the previous round's array, coalesced
     for (unsigned i = start * blockDim.x + threadIdx.x; i < (unsigned)a.nodes; i += stride * blockDim.x)
@@ -1103,9 +1145,12 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
     for (int k = 0; k < kEPT; k++) {
       const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
       in_range[k] = idx < W;
-      e[k] = in_range[k] ? __ldcg(in + seg_at(s, idx)) : make_int4(0, 0, 0, 0);
+      e[k] = in_range[k] ? load_entry(a, in, seg_at(s, idx)) : make_int4(0, 0, 0, 0);
       if (e[k].x < 0) in_range[k] = false;  // null entry (unused scan slot)
     }
+    int4 orig[kEPT];
+#pragma unroll
+    for (int k = 0; k < kEPT; k++) orig[k] = e[k];
     int v[N];
     bool vv[N];
 #pragma unroll
@@ -1123,7 +1168,7 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
 #pragma unroll
       for (int k = 0; k < kEPT; k++) keep[k] = in_range[k];
     } else {
-      multi_find<N>(v, vv, a.parent, s, !(a.abl & kAblNoFindCache));
+      multi_find<N>(v, vv, a.parent, s, !(a.abl & kAblNoFindCache), keep_ends ? 0 : kSplitAfter);
 #pragma unroll
       for (int k = 0; k < kEPT; k++) {
         keep[k] = in_range[k] && v[2 * k] != v[2 * k + 1];
@@ -1132,12 +1177,14 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
       }
       if (dedup) drop_parallel<kEPT>(e, keep, s);  // uniform across the CTA
       unsigned pos = warp_reserve<kEPT>(keep, s, region);
+      if (!count_only) {
 #pragma unroll
-      for (int k = 0; k < kEPT; k++) {
-        if (keep[k]) {
-          if (pos < a.wl_cap) out[pos] = e[k];
-          else atomicOr(&a.st->error, kErrOverflow);
-          pos++;
+        for (int k = 0; k < kEPT; k++) {
+          if (keep[k]) {
+            if (pos < a.wl_cap) store_entry(a, out, pos, keep_ends ? orig[k] : e[k]);
+            else atomicOr(&a.st->error, kErrOverflow);
+            pos++;
+          }
         }
       }
     }
@@ -1183,9 +1230,11 @@ __device__ __forceinline__ void hot_refresh(const u64* mcur, RoundSmem& s) {
 // list is the one the prefix table in `s` describes (W logical entries).
 __device__ __forceinline__ void round_mark(const RoundArgs& a, const int4* wl, unsigned W,
                                            const u64* mcur, unsigned start, unsigned stride,
-                                           const RoundSmem& s) {
+                                           RoundSmem& s) {
+  constexpr int N = 2 * kEPT;
   const unsigned tile = blockDim.x * kEPT;
   const unsigned ntiles = (W + tile - 1) / tile;
+  const bool keep_ends = (a.abl & kAblKeepEnds) != 0;
   for (unsigned t = start; t < ntiles; t += stride) {
     int4 e[kEPT];
     bool in_range[kEPT];
@@ -1193,8 +1242,30 @@ __device__ __forceinline__ void round_mark(const RoundArgs& a, const int4* wl, u
     for (int k = 0; k < kEPT; k++) {
       const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
       in_range[k] = idx < W;
-      e[k] = in_range[k] ? __ldcg(wl + seg_at(s, idx)) : make_int4(0, 0, 0, 0);
+      e[k] = in_range[k] ? load_entry(a, wl, seg_at(s, idx)) : make_int4(0, 0, 0, 0);
       if (e[k].x < 0) in_range[k] = false;  // null entry (unused scan slot)
+    }
+    if (keep_ends) {
+      // Entries hold their endpoints, not reps: find them again. Unions of
+      // this pass may already have moved a root; a key then meets the slot of
+      // the tree it joined, which can only defer an edge to a later round:
+      // every edge marked is still the lightest edge leaving a tree of the
+      // find/min pass (the reference's kernel2 finds the same way, :198-216).
+      int v[N];
+      bool vv[N];
+#pragma unroll
+      for (int k = 0; k < kEPT; k++) {
+        v[2 * k] = e[k].x;
+        v[2 * k + 1] = e[k].y;
+        vv[2 * k] = vv[2 * k + 1] = in_range[k];
+      }
+      multi_find<N>(v, vv, a.parent, s, false, 0);
+#pragma unroll
+      for (int k = 0; k < kEPT; k++) {
+        e[k].x = v[2 * k];
+        e[k].y = v[2 * k + 1];
+        if (e[k].x == e[k].y) in_range[k] = false;
+      }
     }
     u64 mx[kEPT], my[kEPT];
 #pragma unroll
@@ -1230,10 +1301,16 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
   bool tail = false;
   int r = 0;
   const bool stamp = blockIdx.x == 0 && threadIdx.x == 0;
+  // Round 0 offers straight from the scan's list, whose endpoints are roots
+  // (not so under kAblNoTuples: those lists hold CSR indices, whose
+  // endpoints are gathered as they are).
+  const bool fresh0 = !(a.abl & kAblNoTuples);
+  const bool ndd = (a.abl & kAblNoDD) != 0;
   if (stamp) st->t_round_start[ph] = globaltimer_ns();
   for (;;) {
-    const unsigned W = min(ld_volatile(&st->wl_count[ph][r]), a.wl_cap);
-    if (W == 0) break;
+    unsigned W = min(ld_volatile(&st->wl_count[ph][r]), a.wl_cap);
+    if (W == 0) break;  // (kAblNoDD: no entry joined two trees last round)
+    if (ndd) W = min(ld_volatile(&st->wl_count[ph][0]), a.wl_cap);  // the phase's whole list, every round
     if (r >= ECL_MAX_ROUNDS) {
       if (stamp) atomicOr(&st->error, kErrRounds);
       break;
@@ -1243,24 +1320,28 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
       if (blockIdx.x != 0) return;
     }
     const unsigned start = tail ? 0u : blockIdx.x, stride = tail ? 1u : gridDim.x;
-    // Round 0 reads the scan's list (wl0) and keeps it as its output; from
-    // round 1 on the lists alternate. The min-slot arrays alternate per round.
-    const bool fresh = r == 0;
-    const bool in1 = !fresh && ((r - 1) & 1) != 0;
+    // A fresh round 0 reads the scan's list (wl0) and keeps it as its
+    // output; the compacting rounds after it alternate between the lists.
+    // The min-slot arrays alternate per round.
+    const bool fresh = fresh0 && r == 0;
+    const int k = fresh0 ? r - 1 : r;  // index among the compacting rounds
+    const bool in1 = !fresh && !ndd && (k & 1) != 0;
     const int4* in = in1 ? a.wl1 : a.wl0;
     int4* out = in1 ? a.wl0 : a.wl1;
     const bool odd = (r & 1) != 0;
     u64* mcur = odd ? a.minv1 : a.minv0;
     u64* mprev = odd ? a.minv0 : a.minv1;
-    const int reset = fresh ? kResetNone
-                            : (!tail && 4ull * W >= (unsigned long long)a.nodes ? kResetDense : kResetSparse);
+    // entries that keep their endpoints cannot name the previous round's
+    // reps: those rounds clear the whole previous array
+    const bool dense = (a.abl & kAblKeepEnds) || 4ull * W >= (unsigned long long)a.nodes;
+    const int reset = r == 0 ? kResetNone : (!tail && dense ? kResetDense : kResetSparse);
     round_find_min(a, in, W, out, &st->wl_count[ph][r + 1], &st->wl_kept[ph][r + 1], mcur, mprev, reset,
                    fresh, start, stride, s);
     if (fresh && blockIdx.x == 0 && threadIdx.x == 0) {  // the scan's list is round 0's output
       st->wl_count[ph][1] = W;
       st->wl_kept[ph][1] = st->scan_kept[ph];
     }
-    if (!fresh && !tail && threadIdx.x == 0) {  // this CTA's segment of the output list
+    if (!fresh && !tail && !ndd && threadIdx.x == 0) {  // this CTA's segment of the output list
       st->seg_cnt[blockIdx.x] = s.cursor;
       st->seg_off[blockIdx.x] = share_region(W, blockDim.x * kEPT, blockIdx.x, gridDim.x);
     }
@@ -1272,12 +1353,12 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
     if (W2 == 0) break;
     // the list the mark pass and the next round read: the scan's list (round
     // 0), the tail CTA's single segment, or the grid's per-CTA segments
-    if (!fresh) {
+    if (!fresh && !ndd) {
       if (tail) seg_set_dense(s, s.cursor);
       else seg_load(s, st, (int)gridDim.x);
     }
     hot_refresh(mcur, s);
-    round_mark(a, fresh ? in : out, W2, mcur, start, stride, s);
+    round_mark(a, fresh || ndd ? in : out, ndd ? W : W2, mcur, start, stride, s);
     __syncthreads();
     round_smem_clear(s);
     if (tail) __syncthreads();
@@ -1285,6 +1366,102 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
     if (stamp) st->t_round[ph][2 * r - 1] = globaltimer_ns();
   }
   if (stamp) st->rounds[ph] = r;
+}
+
+// ------------------------------------------------ reference ablation steps
+// kAblNoTuples: the vertex of every CSR entry (the reference's NoTuples
+// variant keeps such an slist, Deoptimizations/..._NoTuples.cu:163-169),
+// filled entry-parallel from the scans' tile->vertex table (the row holding
+// entry t * kGran), then a short walk along nindex.
+__global__ void __launch_bounds__(kThreads) k_slist(const int* nindex, const int* first_v, int* slist,
+                                                    int edges, const DevState* st) {
+  if (ld_volatile(&st->error) & kErrFormat) return;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < edges; j += gridDim.x * blockDim.x) {
+    int v = __ldg(first_v + j / kGran);
+    while (__ldg(nindex + v + 1) <= j) v++;
+    slist[j] = v;
+  }
+}
+
+// NoEdgeBased (Deoptimizations/..._NoEdgeBased.cu:152-195): all Boruvka
+// rounds of a phase as vertex-centric passes over the CSR, one thread per
+// vertex walking its row, in one cooperative launch: (A) every one-direction
+// entry of the phase's weight class whose endpoints lie in different trees
+// offers its key to both roots, (B) an entry holding the minimum of either
+// root's slot joins the trees and is marked, (C) the slots are cleared. The
+// rounds end when pass A finds no entry across two trees (the reference's
+// go_again). Pass B finds while other threads join; an entry it marks is
+// still the lightest edge leaving a tree of pass A, so the forest is the
+// reference's (an edge missed in one round is found in a later one).
+__global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds_vertex(RoundArgs a,
+                                                                                       const int* nindex) {
+  DevState* st = a.st;
+  const int ph = a.phase;
+  if (ph == 1 && !st->filtered) return;
+  if (ld_volatile(&st->error) & (kErrFormat | kErrTimeout)) return;
+  const int n = a.nodes, thr = st->threshold;
+  const bool filtered = st->filtered != 0, guard = !(a.abl & kAblNoGuards);
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  u64* mv = a.minv0;
+  const bool stamp = blockIdx.x == 0 && threadIdx.x == 0;
+  if (stamp) st->t_round_start[ph] = globaltimer_ns();
+  auto in_phase = [&](int w) { return !filtered || (ph == 0 ? w <= thr : w > thr); };
+  int r = 0;
+  for (;; r++) {
+    if (r >= ECL_MAX_ROUNDS) {
+      if (stamp) atomicOr(&st->error, kErrRounds);
+      break;
+    }
+    unsigned live = 0;
+    for (int v = gid; v < n; v += gstride) {  // pass A
+      const int beg = __ldg(nindex + v), end = __ldg(nindex + v + 1);
+      int rv = -1;
+      for (int j = beg; j < end; j++) {
+        const int nb = __ldg(a.nlist + j);
+        if (nb <= v) continue;  // one direction
+        const int w = __ldg(a.eweight + j);
+        if (!in_phase(w)) continue;
+        if (rv < 0) rv = find_halve(v, a.parent);
+        const int rn = find_halve(nb, a.parent);
+        if (rv == rn) continue;
+        live++;
+        const u64 key = edge_key(w, j);
+        if (!guard || __ldcg(mv + rv) > key) atomicMin(mv + rv, key);
+        if (!guard || __ldcg(mv + rn) > key) atomicMin(mv + rn, key);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) live += __shfl_xor_sync(0xffffffffu, live, o);
+    if (lane == 0 && live) atomicAdd(&st->wl_count[ph][r + 1], live);
+    if (!grid_barrier(st, kBarrierTimeoutNs)) return;
+    if (stamp) st->t_round[ph][2 * r] = globaltimer_ns();
+    if (ld_volatile(&st->wl_count[ph][r + 1]) == 0) break;
+    for (int v = gid; v < n; v += gstride) {  // pass B
+      const int beg = __ldg(nindex + v), end = __ldg(nindex + v + 1);
+      for (int j = beg; j < end; j++) {
+        const int nb = __ldg(a.nlist + j);
+        if (nb <= v) continue;
+        const int w = __ldg(a.eweight + j);
+        if (!in_phase(w)) continue;
+        const int rv = find_ro(v, a.parent), rn = find_ro(nb, a.parent);
+        if (rv == rn) continue;
+        const u64 key = edge_key(w, j);
+        if (key == __ldcg(mv + rv) || key == __ldcg(mv + rn)) {
+          cas_union(rv, rn, a.parent);
+          a.inMST[j] = 1;
+        }
+      }
+    }
+    if (!grid_barrier(st, kBarrierTimeoutNs)) return;
+    for (int v = gid; v < n; v += gstride) __stcg(mv + v, kNoEdge);  // pass C
+    if (!grid_barrier(st, kBarrierTimeoutNs)) return;
+    if (stamp) st->t_round[ph][2 * r + 1] = globaltimer_ns();
+  }
+  if (stamp) {
+    st->rounds[ph] = r;
+    st->wl_count[ph][0] = st->wl_count[ph][1];
+  }
 }
 
 }  // namespace ecl

@@ -33,6 +33,8 @@ FLAG_L2_PERSIST, FLAG_STATS, FLAG_NO_SMALL_TAIL = 1, 2, 4
 FLAG_NO_GUARDS, FLAG_NO_WARP_COOP, FLAG_DEDUP, FLAG_NO_FIND_CACHE = 8, 16, 32, 64
 # direct launches instead of replaying a captured solve (keeps per-phase timings)
 FLAG_NO_GRAPH = 128
+# the reference's later deoptimization steps (single-graph contexts only)
+FLAG_NO_IMPLICIT_COMPRESSION, FLAG_NO_TUPLES, FLAG_NO_DATA_DRIVEN, FLAG_NO_EDGE_BASED = 256, 512, 1024, 2048
 MAX_ROUNDS = 64
 
 

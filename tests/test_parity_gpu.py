@@ -26,6 +26,16 @@ MODES = [
     dict(flags=E.FLAG_NO_WARP_COOP),
     dict(flags=E.FLAG_DEDUP),
     dict(flags=E.FLAG_NO_FIND_CACHE),
+    dict(flags=E.FLAG_L2_PERSIST),
+    # the reference's later deoptimization steps, alone and stacked
+    dict(flags=E.FLAG_NO_IMPLICIT_COMPRESSION),
+    dict(flags=E.FLAG_NO_TUPLES),
+    dict(flags=E.FLAG_NO_DATA_DRIVEN),
+    dict(flags=E.FLAG_NO_EDGE_BASED),
+    dict(flags=E.FLAG_NO_TUPLES | E.FLAG_NO_DATA_DRIVEN | E.FLAG_NO_FIND_CACHE),
+    dict(flags=E.FLAG_NO_GUARDS | E.FLAG_NO_WARP_COOP | E.FLAG_NO_IMPLICIT_COMPRESSION | E.FLAG_NO_TUPLES
+         | E.FLAG_NO_DATA_DRIVEN | E.FLAG_NO_EDGE_BASED, mode=E.THRESH_NONE),
+    dict(flags=E.FLAG_L2_PERSIST | E.FLAG_NO_GRAPH, mode=E.THRESH_QUANTILE, quantile=0.2),
     dict(flags=E.FLAG_NO_GUARDS | E.FLAG_NO_WARP_COOP | E.FLAG_DEDUP | E.FLAG_NO_FIND_CACHE
          | E.FLAG_NO_SMALL_TAIL, mode=E.THRESH_NONE),
 ]
@@ -300,15 +310,18 @@ def test_cli_variants_and_table_pipeline(tmp_path):
     path = str(tmp_path / "rmat14.egr")
     E.write_graph(g, path)
     outs, forests = {}, set()
-    for v in ("base", "NAG", "NAG_NW", "NAG_NW_NF"):
+    # the reference's variant chain (generate_deoptimize_tables.py:6-14)
+    for v in ("base", "NAG", "NAG_NW", "NAG_NW_NF", "NAG_NW_NF_NIPC", "NAG_NW_NF_NIPC_NOD",
+              "NAG_NW_NF_NIPC_NOD_NT", "NAG_NW_NF_NIPC_NOD_NT_NDD", "NAG_NW_NF_NIPC_NOD_NT_NDD_NEB"):
         r = subprocess.run([exe, path, "3", v], capture_output=True, text=True, timeout=120)
         assert r.returncode == 0, r.stderr
+        assert ("NOD" in v) == ("NOD is not reproduced" in r.stderr)
         outs[f"ecl_mst_{v}_out.csv"] = r.stdout
         forests.add(r.stdout.strip().splitlines()[-1])
     assert len(forests) == 1
     inputs, names, rt, tp = T.tables(outs, runs=3)
     assert len(inputs) == 1 and all(x is not None and x > 0 for x in tp[0])
-    r = subprocess.run([exe, path, "3", "NAG_NW_NF_NIPC"], capture_output=True, text=True, timeout=60)
+    r = subprocess.run([exe, path, "3", "NAG_XYZ"], capture_output=True, text=True, timeout=60)
     assert r.returncode != 0
 
 
