@@ -50,6 +50,7 @@ constexpr int kGran = 128;             // entries per tile->vertex table step (t
 #define ECL_PAIR_LOG 10
 #endif
 constexpr int kRoundThreads = ECL_ROUND_THREADS;  // threads of a round CTA (one worklist entry each per tile)
+static_assert(2 * kRoundThreads >= kMaxRoundCtas, "seg_load: two segments per thread of a round CTA");
 #ifndef ECL_ROUND_EPT
 #define ECL_ROUND_EPT 1
 #endif
@@ -793,38 +794,34 @@ __device__ __forceinline__ void seg_set_dense(RoundSmem& s, unsigned count) {
 }
 
 // The list read next is the one the grid's find/min pass just wrote (`nseg`
-// segments, published in the control block before the grid barrier). One
-// warp builds the prefix table; the caller synchronises the CTA before use.
+// segments, published in the control block before the grid barrier). The
+// whole CTA builds the prefix table: thread t loads segments 2t and 2t + 1
+// (nseg <= kMaxRoundCtas = 2 x the round CTA's threads), one warp scan and
+// one pass over the warp totals give the prefixes. Every thread of the CTA
+// must call this; the caller synchronises the CTA before the table is used.
 __device__ __forceinline__ void seg_load(RoundSmem& s, const DevState* st, int nseg) {
-  if (threadIdx.x >= 32) return;
-  const int lane = threadIdx.x;
-  const int per = (nseg + 31) >> 5;
-  const int b0 = lane * per;
-  unsigned sum = 0;
-  for (int k = 0; k < per; k++) {
-    const int b = b0 + k;
-    if (b < nseg) {
-      const unsigned c = __ldcg(&st->seg_cnt[b]);
-      s.seg_off[b] = __ldcg(&st->seg_off[b]);
-      s.seg_q[b] = sum;
-      sum += c;
-    }
-  }
-  unsigned incl = sum;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int b0 = 2 * t, b1 = 2 * t + 1;
+  const unsigned c0 = b0 < nseg ? __ldcg(&st->seg_cnt[b0]) : 0u;
+  const unsigned c1 = b1 < nseg ? __ldcg(&st->seg_cnt[b1]) : 0u;
+  if (b0 < nseg) s.seg_off[b0] = __ldcg(&st->seg_off[b0]);
+  if (b1 < nseg) s.seg_off[b1] = __ldcg(&st->seg_off[b1]);
+  const unsigned mine = c0 + c1;
+  unsigned incl = mine;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += t;
+    const unsigned x = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += x;
   }
-  const unsigned excl = incl - sum;
-  for (int k = 0; k < per; k++) {
-    const int b = b0 + k;
-    if (b < nseg) s.seg_q[b] += excl;
-  }
-  if (lane == 31) {
-    s.seg_q[nseg] = incl;
-    s.seg_n = nseg;
-  }
+  if (lane == 31) s.rs.warp_off[warp][0] = incl;
+  __syncthreads();
+  unsigned before = 0;
+  for (int w = 0; w < warp; w++) before += s.rs.warp_off[w][0];
+  const unsigned excl = before + incl - mine;
+  if (b0 < nseg) s.seg_q[b0] = excl;
+  if (b1 < nseg) s.seg_q[b1] = excl + c0;
+  if (b0 < nseg && nseg <= b1 + 1) s.seg_q[nseg] = excl + mine;  // the thread holding the last segment
+  if (t == 0) s.seg_n = nseg;
 }
 
 // Position of logical entry i of the list described by the prefix table.

@@ -1,28 +1,35 @@
 """Training pipeline of the learned schedule (runs on a GPU).
 
-1. Generate seeded training and held-out graphs from the four families
-   (2D grid, Erdos-Renyi avg degree 8-32, RMAT (.57,.19,.19) edge factor 8-32,
-   random geometric 2D avg degree 3), vertex counts log-uniform in
-   [--nmin, --nmax].
-2. Label sweep: solve every graph with each of 16 filter quantiles x 6 degree
-   splits (device time, best of --reps runs) and take the fastest setting
-   as the label (log2 quantile, log2 split). The sweep uses the engine's own
-   schedules; every setting gives the same forest.
-3. Train the 16 -> 64 -> 64 -> 2 MLP with the library's CUDA training kernel
-   (Adam, one launch) on standardised features.
-4. Evaluate on the held-out graphs: device time of the learned schedule vs
-   the reference heuristic (its fallback and judge) vs the best of the sweep.
-5. Write the parameter blob (filter_weights.bin, next to this file unless
-   --out says otherwise) and a JSON summary.
+1. Draw seeded training and held-out graphs on the device (the library's
+   device generators) from the four families: 2D grid, Erdos-Renyi (average
+   degree 8, 16 or 32), RMAT (.57, .19, .19; edge factor 8, 16 or 32) and
+   random geometric 2D (average degree 3), vertex counts log-uniform in
+   [--nmin, --nmax], weights uniform in [1, W] with W one of 2^20, 2^24, 2^30.
+2. Label sweep: solve every graph with each of 16 filter quantiles x the 3
+   distinct degree splits (the scans' entries per lane E = 4, 8, 16; larger
+   splits select the same schedule) and keep the device times (best of
+   --reps timed runs after one warm-up; repeated solves replay their captured
+   CUDA graph). Every setting gives the same forest.
+3. Label each graph with a soft minimum over the sweep (log2 quantile
+   relative to the reference heuristic's, log2 split) and train the
+   16 -> 64 -> 64 -> 2 MLP with the library's CUDA training kernel (Adam, one
+   launch) on standardised features, graphs weighted by their solve time.
+4. Evaluate on the held-out seeds: the sweep time at the predicted setting
+   against the reference heuristic (its fallback and judge) and the best of
+   the sweep, per family; then re-solve every held-out graph with the trained
+   weights loaded, learned against heuristic, and report the measured gain
+   and the share of graphs that are not slower.
+5. Write the parameter blob (filter_weights.bin) and the JSON summary
+   (filter_training.json) into --out-dir; with --dataset, also the sweep
+   tables.
 
-    python train_filter.py --train 600 --heldout 100 --out-dir <dir>
+    python train_filter.py --train 2000 --heldout 500 --out-dir <dir>
 """
 import argparse
 import json
 import os
 import sys
 import time
-from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -31,45 +38,48 @@ sys.path.insert(0, HERE)
 import ecl_mst as E  # noqa: E402
 
 QUANTILES = [0.005, 0.01, 0.02, 0.03, 0.05, 0.07, 0.1, 0.15, 0.2, 0.3, 0.4, 0.5, 0.65, 0.8, 0.9, 1.0]
-SPLITS = [2, 4, 8, 16, 32, 64]
+SPLITS = [4, 8, 16]  # degree splits selecting the scans' E = 4, 8, 16 entries per lane
+FAMILIES = ["grid", "er", "rmat", "rgg"]
+TRAIN_SEED0, HELDOUT_SEED0 = 200_000, 900_000
 
 
 def make_graph(seed, nmin, nmax):
+    """(DeviceGraph, family name) of training or held-out seed `seed`."""
     rng = np.random.default_rng(seed)
     fam = int(rng.integers(4))
     n = int(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
+    wmax = int(rng.choice([1 << 20, 1 << 24, 1 << 30]))
     if fam == 0:
         r = max(2, int(np.sqrt(n)))
-        return E.gen_grid(r, max(2, n // r), seed, 1 << 24, threads=2), "grid"
+        return E.gen_grid_device(r, max(2, n // r), seed, wmax), "grid"
     if fam == 1:
-        return E.gen_er(n, float(rng.choice([8, 16, 32])), seed, 1 << 24, threads=2), "er"
+        return E.gen_er_device(n, float(rng.choice([8, 16, 32])), seed, wmax), "er"
     if fam == 2:
-        return E.gen_rmat(max(10, int(round(np.log2(n)))), int(rng.choice([8, 16, 32])), 0.57, 0.19, 0.19, seed,
-                          1 << 24, threads=2), "rmat"
-    return E.gen_rgg2d(n, 3.0, seed, 1 << 24, threads=2), "rgg"
+        return E.gen_rmat_device(max(10, int(round(np.log2(n)))), int(rng.choice([8, 16, 32])), 0.57, 0.19, 0.19,
+                                 seed, wmax), "rmat"
+    return E.gen_rgg2d_device(n, 3.0, seed, wmax), "rgg"
 
 
-def sweep(ctx, g, torch, dev, reps):
-    ni, nl, ew = (torch.from_numpy(a).to(dev) for a in (g.nindex, g.nlist, g.eweight))
-    out = torch.empty(max(g.edges, 1), dtype=torch.uint8, device=dev)
-    feat = E.graph_features(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), ew.data_ptr())
+def solve_ms(ctx, dg, out, opts, reps):
+    """Best device time of `reps` timed solves after one warm-up."""
+    best = 1e30
+    for r in range(reps + 1):
+        st = ctx.run_device(dg.nodes, dg.edges, dg.d_nindex, dg.d_nlist, dg.d_eweight, out.data_ptr(), opts=opts,
+                            stats=True)
+        if r > 0:
+            best = min(best, st["ms_total"])
+    return best
 
-    def timed(opts):
-        best = 1e30
-        for r in range(reps + 1):
-            st = ctx.run_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(),
-                                opts=opts, stats=True)
-            if r > 0:
-                best = min(best, st["ms_total"])
-        return best
 
+def sweep(ctx, dg, out, reps):
+    feat = E.graph_features(dg.nodes, dg.edges, dg.d_nindex, dg.d_nlist, dg.d_eweight)
     times = np.zeros((len(QUANTILES), len(SPLITS)), np.float32)
     for qi, q in enumerate(QUANTILES):
         for si, sp in enumerate(SPLITS):
-            times[qi, si] = timed(E.make_opts(mode=E.THRESH_QUANTILE, quantile=q, degree_split=sp))
-    heur = timed(E.make_opts())
-    learned = timed(E.make_opts(mode=E.THRESH_LEARNED)) if E.learned_load_default() else None
-    return feat, times, heur, learned
+            times[qi, si] = solve_ms(ctx, dg, out, E.make_opts(mode=E.THRESH_QUANTILE, quantile=q, degree_split=sp),
+                                     reps)
+    heur = solve_ms(ctx, dg, out, E.make_opts(), reps)
+    return feat, times, heur
 
 
 def heuristic_log2_quantile(n, m):
@@ -94,29 +104,44 @@ def label(times, n, m, tau=0.03):
                     np.float32)
 
 
+def predicted_setting(pr, n, m):
+    """Grid point nearest the MLP's output (as the device applies it)."""
+    lq = min(max(heuristic_log2_quantile(n, m) + float(pr[0]), -10.0), 0.0)
+    q = 1.0 if lq >= -0.02 else 2.0 ** lq
+    sp = int(round(min(max(float(pr[1]), 1.0), 6.0)))
+    qi = int(np.argmin([abs(np.log2(a) - np.log2(q)) for a in QUANTILES]))
+    si = 0 if sp <= 2 else (1 if sp == 3 else 2)  # E = 4 for splits <= 4, 8 for 8, 16 above
+    return qi, si
+
+
+def collect(ctx, count, seed0, nmin, nmax, reps, torch):
+    rows = []
+    t0 = time.time()
+    for i in range(count):
+        dg, fam = make_graph(seed0 + i, nmin, nmax)
+        out = torch.empty(max(dg.edges, 1), dtype=torch.uint8, device="cuda:0")
+        f, tm, h = sweep(ctx, dg, out, reps)
+        rows.append(dict(x=f, times=tm, heur=h, fam=fam, size=(dg.nodes, dg.edges)))
+        dg.close()
+        del out
+        if (i + 1) % 100 == 0:
+            print(f"  {i + 1}/{count} graphs swept, {time.time() - t0:.0f} s", flush=True)
+    return dict(x=np.array([r["x"] for r in rows]), times=np.array([r["times"] for r in rows]),
+                heur=np.array([r["heur"] for r in rows]), fam=[r["fam"] for r in rows],
+                size=np.array([r["size"] for r in rows]))
+
+
 def run(args):
     import torch
-    dev = torch.device("cuda:0")
-    ctx = E.Context(args.nmax * 2, args.nmax * 130)
-    data = {}
-    for split_name, count, base in (("train", args.train, 200000), ("heldout", args.heldout, 900000)):
-        feats, times, heurs, fams, sizes = [], [], [], [], []
-        t0 = time.time()
-        with ThreadPoolExecutor(max(1, (os.cpu_count() or 2) // 2)) as ex:
-            futs = [ex.submit(make_graph, base + i, args.nmin, args.nmax) for i in range(count)]
-            for i, fu in enumerate(futs):
-                g, fam = fu.result()
-                futs[i] = None
-                f, tm, h, _ = sweep(ctx, g, torch, dev, args.reps)
-                sizes.append((g.nodes, g.edges))
-                feats.append(f)
-                times.append(tm)
-                heurs.append(h)
-                fams.append(fam)
-        print(f"{split_name}: {count} graphs swept in {time.time() - t0:.0f} s", flush=True)
-        data[split_name] = dict(x=np.array(feats), times=np.array(times), heur=np.array(heurs), fam=fams,
-                                size=np.array(sizes))
-    tr = data["train"]
+    # largest graphs drawn: RMAT scale 22 at edge factor 32, ER n_max at degree 32
+    ctx = E.Context(1 << 23, 300_000_000)
+    t0 = time.time()
+    tr = collect(ctx, args.train, TRAIN_SEED0, args.nmin, args.nmax, args.reps, torch)
+    print(f"train: {args.train} graphs swept in {time.time() - t0:.0f} s", flush=True)
+    t0 = time.time()
+    ho = collect(ctx, args.heldout, HELDOUT_SEED0, args.nmin, args.nmax, args.reps, torch)
+    print(f"heldout: {args.heldout} graphs swept in {time.time() - t0:.0f} s", flush=True)
+
     x = tr["x"]
     mean, std = x.mean(0), x.std(0) + 1e-6
     y = np.stack([label(t, n, m) for t, (n, m) in zip(tr["times"], tr["size"])])
@@ -127,51 +152,67 @@ def run(args):
     ys = np.repeat(y, rep, 0)[order]
     p0 = E.mlp_init(args.seed, mean=mean, std=std)
     p, hist = E.mlp_train(p0, xs, ys, epochs=args.epochs, lr=args.lr)
-    # held-out evaluation from the sweep table: time at the predicted grid point
-    ho = data["heldout"]
+
+    # held-out, from the sweep tables: time at the predicted grid point
     pred = E.mlp_forward(p, ho["x"])
     res = []
     for pr, tm, h, (n, m) in zip(pred, ho["times"], ho["heur"], ho["size"]):
-        lq = min(max(heuristic_log2_quantile(n, m) + float(pr[0]), -10.0), 0.0)
-        q = 1.0 if lq >= -0.02 else 2.0 ** lq
-        sp = 1 << int(round(min(max(float(pr[1]), 1.0), 6.0)))
-        qi = int(np.argmin([abs(np.log2(a) - np.log2(q)) for a in QUANTILES]))
-        si = SPLITS.index(sp) if sp in SPLITS else 2
+        qi, si = predicted_setting(pr, n, m)
         res.append((float(tm[qi, si]), float(h), float(tm.min())))
     res = np.array(res)
+    fams = np.array(ho["fam"])
+    gated = ho["size"][:, 1] >= (1 << 20)  # graphs the library runs the learned schedule on
+
+    def gain(sel):
+        return {"graphs": int(sel.sum()), "ms_learned": float(res[sel, 0].sum()),
+                "ms_heuristic": float(res[sel, 1].sum()), "ms_best": float(res[sel, 2].sum()),
+                "gain_over_heuristic": float(res[sel, 1].sum() / max(res[sel, 0].sum(), 1e-9)),
+                "not_slower": float((res[sel, 0] <= res[sel, 1] * 1.02).mean()) if sel.any() else None}
+
     summary = {
         "train_graphs": args.train, "heldout_graphs": args.heldout, "nmin": args.nmin, "nmax": args.nmax,
-        "quantiles": QUANTILES, "splits": SPLITS, "epochs": args.epochs, "lr": args.lr,
+        "train_seeds": [TRAIN_SEED0, TRAIN_SEED0 + args.train - 1],
+        "heldout_seeds": [HELDOUT_SEED0, HELDOUT_SEED0 + args.heldout - 1],
+        "quantiles": QUANTILES, "splits": SPLITS, "reps": args.reps, "epochs": args.epochs, "lr": args.lr,
         "loss_first": float(hist[0]), "loss_last": float(hist[-1]),
-        "heldout_ms_learned": float(res[:, 0].sum()), "heldout_ms_heuristic": float(res[:, 1].sum()),
-        "heldout_ms_best": float(res[:, 2].sum()),
-        "heldout_gain_over_heuristic": float(res[:, 1].sum() / res[:, 0].sum()),
-        "heldout_graphs_not_slower": float((res[:, 0] <= res[:, 1] * 1.02).mean()),
-        "train_label_quantiles": {str(q): int((np.abs(y[:, 0] - np.log2(q)) < 1e-6).sum()) for q in QUANTILES},
-        "train_label_splits": {str(s): int((np.abs(y[:, 1] - np.log2(s)) < 1e-6).sum()) for s in SPLITS},
+        "sweep_heldout": gain(np.ones(len(res), bool)),
+        "sweep_heldout_by_family": {f: gain(fams == f) for f in FAMILIES},
+        "sweep_heldout_learned_size": gain(gated),
     }
+
     # measured: re-solve the held-out graphs with the trained weights loaded
     E.learned_set_weights(p)
-    t_h = t_l = 0.0
+    meas = []
     for i in range(args.heldout):
-        g, _ = make_graph(900000 + i, args.nmin, args.nmax)
-        ni, nl, ew = (torch.from_numpy(a).to(dev) for a in (g.nindex, g.nlist, g.eweight))
-        out = torch.empty(max(g.edges, 1), dtype=torch.uint8, device=dev)
-        for mode in (E.THRESH_HEURISTIC, E.THRESH_LEARNED, E.THRESH_HEURISTIC, E.THRESH_LEARNED):
-            ts = [ctx.run_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(),
-                                 opts=E.make_opts(mode=mode), stats=True)["ms_total"] for _ in range(3)]
-            if mode == E.THRESH_HEURISTIC:
-                t_h += min(ts[1:]) / 2
-            else:
-                t_l += min(ts[1:]) / 2
+        dg, fam = make_graph(HELDOUT_SEED0 + i, args.nmin, args.nmax)
+        out = torch.empty(max(dg.edges, 1), dtype=torch.uint8, device="cuda:0")
+        th = tl = 1e30
+        for _ in range(2):  # interleaved, best of each
+            th = min(th, solve_ms(ctx, dg, out, E.make_opts(mode=E.THRESH_HEURISTIC), args.reps))
+            tl = min(tl, solve_ms(ctx, dg, out, E.make_opts(mode=E.THRESH_LEARNED), args.reps))
+        meas.append((fam, dg.edges, th, tl))
+        dg.close()
+        del out
     ctx.close()
-    summary["heldout_measured_ms_heuristic"] = t_h
-    summary["heldout_measured_ms_learned"] = t_l
-    summary["heldout_measured_gain"] = t_h / t_l
+
+    def mgain(sel):
+        th = sum(t for (f, m, t, _), s in zip(meas, sel) if s)
+        tl = sum(t for (f, m, _, t), s in zip(meas, sel) if s)
+        ns = [tl_ <= th_ * 1.02 for (f, m, th_, tl_), s in zip(meas, sel) if s]
+        return {"graphs": int(sum(sel)), "ms_heuristic": th, "ms_learned": tl, "gain": th / max(tl, 1e-9),
+                "not_slower": float(np.mean(ns)) if ns else None}
+
+    big = [m >= (1 << 20) for (_, m, _, _) in meas]
+    summary["measured_heldout"] = mgain([True] * len(meas))
+    summary["measured_heldout_learned_size"] = mgain(big)
+    summary["measured_heldout_by_family"] = {f: mgain([fm == f and b for (fm, _, _, _), b in zip(meas, big)])
+                                             for f in FAMILIES}
     os.makedirs(args.out_dir, exist_ok=True)
     np.asarray(p, np.float32).tofile(os.path.join(args.out_dir, "filter_weights.bin"))
-    np.savez_compressed(os.path.join(args.out_dir, "filter_dataset.npz"), train_x=tr["x"], train_times=tr["times"],
-                        train_heur=tr["heur"], heldout_x=ho["x"], heldout_times=ho["times"], heldout_heur=ho["heur"])
+    if args.dataset:
+        np.savez_compressed(args.dataset, train_x=tr["x"], train_times=tr["times"], train_heur=tr["heur"],
+                            train_size=tr["size"], heldout_x=ho["x"], heldout_times=ho["times"],
+                            heldout_heur=ho["heur"], heldout_size=ho["size"])
     with open(os.path.join(args.out_dir, "filter_training.json"), "w") as f:
         json.dump(summary, f, indent=1)
     print(json.dumps(summary), flush=True)
@@ -179,13 +220,14 @@ def run(args):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--train", type=int, default=600)
-    ap.add_argument("--heldout", type=int, default=100)
+    ap.add_argument("--train", type=int, default=2000)
+    ap.add_argument("--heldout", type=int, default=500)
     ap.add_argument("--nmin", type=int, default=10_000)
     ap.add_argument("--nmax", type=int, default=4_000_000)
-    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--epochs", type=int, default=150)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out-dir", default=HERE)
+    ap.add_argument("--dataset", default=None, help="also write the sweep tables (.npz) here")
     run(ap.parse_args())

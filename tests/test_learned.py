@@ -109,30 +109,28 @@ def test_learned_mode_keeps_the_answer(golden):
 
 @pytest.mark.gpu
 def test_trained_network_gains_over_the_heuristic():
-    """Held-out graphs (seeds never used in training): device time of the
-    learned schedule against the reference heuristic's, same answers."""
+    """Held-out graphs (seeds the training never drew, train_filter.py's
+    held-out range) of 200k-4M vertices from the four families: the learned
+    schedule solves them faster than the reference heuristic in total, with
+    the same answers. Each graph is timed best of three, the two schedules
+    interleaved."""
     if not E.learned_load_default():
         pytest.skip("no trained weights shipped")
     import torch
-    dev = torch.device("cuda:0")
-    graphs = [E.gen_rmat(20, 16, 0.57, 0.19, 0.19, 900001, 1 << 24), E.gen_er(1 << 20, 24, 900002, 1 << 24),
-              E.gen_rmat(19, 32, 0.57, 0.19, 0.19, 900003, 1 << 24)]
-    ctx = E.Context(max(g.nodes for g in graphs), max(g.edges for g in graphs))
+    import train_filter as TF
     t_h = t_l = 0.0
-    for g in graphs:
-        ni, nl, ew = (torch.from_numpy(a).to(dev) for a in (g.nindex, g.nlist, g.eweight))
-        out = torch.empty(g.edges, dtype=torch.uint8, device=dev)
-        res = {}
-        for mode in (E.THRESH_HEURISTIC, E.THRESH_LEARNED):
-            ts = []
-            for _ in range(5):
-                st = ctx.run_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(),
-                                    opts=E.make_opts(mode=mode), stats=True)
-                ts.append(st["ms_total"])
-            res[mode] = (float(np.median(ts[1:])), out.cpu().numpy().copy())
-        assert np.array_equal(res[E.THRESH_HEURISTIC][1], res[E.THRESH_LEARNED][1])
-        t_h += res[E.THRESH_HEURISTIC][0]
-        t_l += res[E.THRESH_LEARNED][0]
-    print(f"held-out: heuristic {t_h:.3f} ms, learned {t_l:.3f} ms, gain {t_h / t_l:.2f}x")
-    assert t_l <= 1.05 * t_h
-    ctx.close()
+    with E.Context(1 << 23, 300_000_000) as ctx:
+        for i in range(12):
+            dg, fam = TF.make_graph(TF.HELDOUT_SEED0 + i, 200_000, 4_000_000)
+            out = torch.empty(max(dg.edges, 1), dtype=torch.uint8, device="cuda:0")
+            best, answer = {}, {}
+            for _ in range(2):
+                for mode in (E.THRESH_HEURISTIC, E.THRESH_LEARNED):
+                    best[mode] = min(best.get(mode, 1e30), TF.solve_ms(ctx, dg, out, E.make_opts(mode=mode), 1))
+                    answer[mode] = out[: dg.edges].cpu().numpy().copy()
+            assert np.array_equal(answer[E.THRESH_HEURISTIC], answer[E.THRESH_LEARNED]), (i, fam)
+            t_h += best[E.THRESH_HEURISTIC]
+            t_l += best[E.THRESH_LEARNED]
+            dg.close()
+    print(f"held-out: heuristic {t_h:.3f} ms, learned {t_l:.3f} ms, gain {t_h / t_l:.3f}x")
+    assert t_h / t_l > 1.0
