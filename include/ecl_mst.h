@@ -241,8 +241,12 @@ typedef struct mst_opts {
                           /* split <= 4, 8 for split <= 8, else 16; rows       */
                           /* shorter than E stay in one thread, longer rows    */
                           /* are spread over threads/warps; 0 = default (8)    */
-  int32_t block_size;     /* threads per CTA of the round kernel, 0 = default  */
-  int32_t ctas_per_sm;    /* 0 = as many as fit                                */
+  int32_t round_min_tiles; /* the round kernel keeps one CTA per this many   */
+                          /* 512-entry tiles of a round's worklist: CTAs       */
+                          /* beyond it leave the launch as the rounds shrink,  */
+                          /* and its grid barriers wait for the rest only;     */
+                          /* 0 = default (1), < 0 = keep every CTA             */
+  int32_t ctas_per_sm;    /* round-kernel CTAs per SM, 0 = as many as fit      */
   int32_t small_tail;     /* worklist size at which one CTA finishes the      */
                           /* rounds alone; 0 = default, < 0 = never            */
   int32_t flags;          /* ECL_FLAG_*                                        */

@@ -21,6 +21,7 @@ using namespace ecl;
 namespace {
 constexpr int kDefaultSplit = 8;
 constexpr unsigned kDefaultSmallTail = 4096;
+constexpr int kDefaultMinTiles = 1;  // round CTAs kept: one per tile of the round's worklist
 constexpr int64_t kWlSlack = 1 << 19;  // worklist slots beyond `edges` (scan chunk tails)
 constexpr int kLearnedMinEdges = 1 << 20;
 }  // namespace
@@ -511,7 +512,10 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   // entries that keep their endpoints clear the whole previous min array
   // each round, which one CTA of a small tail would do alone
   if (ra.abl & kAblKeepEnds) ra.small_tail = 0;
-  const int rgrid = std::max(1, std::min(c->round_grid, (m / 2 + kRoundThreads - 1) / kRoundThreads + 1));
+  ra.min_tiles = o->round_min_tiles < 0 ? 0 : (o->round_min_tiles == 0 ? kDefaultMinTiles : o->round_min_tiles);
+  int rmax = c->round_grid;
+  if (o->ctas_per_sm > 0) rmax = std::min(rmax, o->ctas_per_sm * c->sm_count);
+  const int rgrid = std::max(1, std::min(rmax, (m / 2 + kRoundThreads - 1) / kRoundThreads + 1));
   if (o->flags & ECL_FLAG_NO_EDGE_BASED) {
     // vertex-centric rounds straight over the CSR: no scans, no worklists
     if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[5], s));
@@ -624,6 +628,7 @@ int check_opts(const mst_opts* o) {
   if (o->threshold_mode < ECL_THRESH_HEURISTIC || o->threshold_mode > ECL_THRESH_LEARNED)
     return ECL_ERR_INVALID_ARG;
   if (o->degree_split < 0 || o->degree_split > (1 << 20)) return ECL_ERR_INVALID_ARG;
+  if (o->ctas_per_sm < 0) return ECL_ERR_INVALID_ARG;
   if (o->threshold_mode == ECL_THRESH_QUANTILE && !(o->quantile >= 0.0f)) return ECL_ERR_INVALID_ARG;
   return ECL_OK;
 }

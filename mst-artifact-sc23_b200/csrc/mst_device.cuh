@@ -119,6 +119,7 @@ struct RoundArgs {
   unsigned small_tail;
   int count_atomics;
   unsigned abl;  // kAbl* bits: techniques switched off to measure what they buy
+  int min_tiles;  // keep one CTA per this many tiles of a round (0 = every CTA)
   // kAblNoTuples: the CSR and the vertex of every entry
   const int* nlist;
   const int* eweight;
@@ -1295,7 +1296,8 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
   round_smem_clear(s);
   seg_set_dense(s, 0);  // round 0 reads the scan's list as it is
   __syncthreads();
-  bool tail = false;
+  unsigned active = gridDim.x;  // CTAs still in the launch
+  bool tail = active == 1;      // one CTA: CTA barriers stand for the grid's
   int r = 0;
   const bool stamp = blockIdx.x == 0 && threadIdx.x == 0;
   // Round 0 offers straight from the scan's list, whose endpoints are roots
@@ -1312,11 +1314,21 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
       if (stamp) atomicOr(&st->error, kErrRounds);
       break;
     }
-    if (!tail && W <= a.small_tail) {
-      tail = true;
-      if (blockIdx.x != 0) return;
+    // CTAs the round keeps: one per min_tiles tiles of its worklist (the
+    // rest leave for good; worklists never grow), or one CTA alone at the
+    // small tail, which then syncs with CTA barriers only
+    unsigned want = active;
+    if (a.min_tiles > 0) {
+      const unsigned per = (unsigned)a.min_tiles * blockDim.x * kEPT;
+      want = min(want, max(1u, (W + per - 1) / per));
     }
-    const unsigned start = tail ? 0u : blockIdx.x, stride = tail ? 1u : gridDim.x;
+    if (W <= a.small_tail) want = 1;
+    if (want < active) {
+      active = want;
+      if (blockIdx.x >= active) return;
+      tail = active == 1;
+    }
+    const unsigned start = blockIdx.x, stride = active;
     // A fresh round 0 reads the scan's list (wl0) and keeps it as its
     // output; the compacting rounds after it alternate between the lists.
     // The min-slot arrays alternate per round.
@@ -1330,8 +1342,8 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
     u64* mprev = odd ? a.minv0 : a.minv1;
     // entries that keep their endpoints cannot name the previous round's
     // reps: those rounds clear the whole previous array
-    const bool dense = (a.abl & kAblKeepEnds) || 4ull * W >= (unsigned long long)a.nodes;
-    const int reset = r == 0 ? kResetNone : (!tail && dense ? kResetDense : kResetSparse);
+    const bool dense = (a.abl & kAblKeepEnds) || (!tail && 4ull * W >= (unsigned long long)a.nodes);
+    const int reset = r == 0 ? kResetNone : (dense ? kResetDense : kResetSparse);
     round_find_min(a, in, W, out, &st->wl_count[ph][r + 1], &st->wl_kept[ph][r + 1], mcur, mprev, reset,
                    fresh, start, stride, s);
     if (fresh && blockIdx.x == 0 && threadIdx.x == 0) {  // the scan's list is round 0's output
@@ -1340,10 +1352,10 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
     }
     if (!fresh && !tail && !ndd && threadIdx.x == 0) {  // this CTA's segment of the output list
       st->seg_cnt[blockIdx.x] = s.cursor;
-      st->seg_off[blockIdx.x] = share_region(W, blockDim.x * kEPT, blockIdx.x, gridDim.x);
+      st->seg_off[blockIdx.x] = share_region(W, blockDim.x * kEPT, start, stride);
     }
     if (tail) __syncthreads();
-    else if (!grid_barrier(st, kBarrierTimeoutNs)) return;
+    else if (!grid_barrier(st, kBarrierTimeoutNs, active)) return;
     if (stamp) st->t_round[ph][2 * r] = globaltimer_ns();
     const unsigned W2 = min(ld_volatile(&st->wl_count[ph][r + 1]), a.wl_cap);
     r++;
@@ -1352,14 +1364,14 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
     // 0), the tail CTA's single segment, or the grid's per-CTA segments
     if (!fresh && !ndd) {
       if (tail) seg_set_dense(s, s.cursor);
-      else seg_load(s, st, (int)gridDim.x);
+      else seg_load(s, st, (int)active);
     }
     hot_refresh(mcur, s);
     round_mark(a, fresh || ndd ? in : out, ndd ? W : W2, mcur, start, stride, s);
     __syncthreads();
     round_smem_clear(s);
     if (tail) __syncthreads();
-    else if (!grid_barrier(st, kBarrierTimeoutNs)) return;
+    else if (!grid_barrier(st, kBarrierTimeoutNs, active)) return;
     if (stamp) st->t_round[ph][2 * r - 1] = globaltimer_ns();
   }
   if (stamp) st->rounds[ph] = r;
@@ -1431,7 +1443,7 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds_
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) live += __shfl_xor_sync(0xffffffffu, live, o);
     if (lane == 0 && live) atomicAdd(&st->wl_count[ph][r + 1], live);
-    if (!grid_barrier(st, kBarrierTimeoutNs)) return;
+    if (!grid_barrier(st, kBarrierTimeoutNs, gridDim.x)) return;
     if (stamp) st->t_round[ph][2 * r] = globaltimer_ns();
     if (ld_volatile(&st->wl_count[ph][r + 1]) == 0) break;
     for (int v = gid; v < n; v += gstride) {  // pass B
@@ -1450,9 +1462,9 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds_
         }
       }
     }
-    if (!grid_barrier(st, kBarrierTimeoutNs)) return;
+    if (!grid_barrier(st, kBarrierTimeoutNs, gridDim.x)) return;
     for (int v = gid; v < n; v += gstride) __stcg(mv + v, kNoEdge);  // pass C
-    if (!grid_barrier(st, kBarrierTimeoutNs)) return;
+    if (!grid_barrier(st, kBarrierTimeoutNs, gridDim.x)) return;
     if (stamp) st->t_round[ph][2 * r + 1] = globaltimer_ns();
   }
   if (stamp) {

@@ -66,17 +66,18 @@ __device__ __forceinline__ unsigned ld_volatile(const unsigned* p) {
   return *(const volatile unsigned*)p;
 }
 
-// Grid-wide barrier for cooperative launches. Every wait is bounded by
-// `timeout_ns`; on expiry the kErrTimeout bit is set and all later barriers
-// return at once, so a stuck CTA turns into an error status instead of a hang.
-// Returns false once the timeout bit is set.
-__device__ __forceinline__ bool grid_barrier(DevState* st, u64 timeout_ns) {
+// Grid-wide barrier for cooperative launches among the `expected` CTAs
+// still in the launch (the others have left for good). Every wait is bounded
+// by `timeout_ns`; on expiry the kErrTimeout bit is set and all later
+// barriers return at once, so a stuck CTA turns into an error status instead
+// of a hang. Returns false once the timeout bit is set.
+__device__ __forceinline__ bool grid_barrier(DevState* st, u64 timeout_ns, unsigned expected) {
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned gen = ld_volatile(&st->bar_gen);
     __threadfence();
     const unsigned arrived = atomicAdd(&st->bar_count, 1u);
-    if (arrived == gridDim.x - 1) {
+    if (arrived == expected - 1) {
       atomicExch(&st->bar_count, 0u);
       __threadfence();
       atomicAdd(&st->bar_gen, 1u);

@@ -20,6 +20,10 @@ MODES = [
     dict(degree_split=1 << 20),
     dict(small_tail=-1),
     dict(small_tail=1 << 30),
+    dict(round_min_tiles=-1),
+    dict(round_min_tiles=16, small_tail=-1),
+    dict(ctas_per_sm=1),
+    dict(ctas_per_sm=1, round_min_tiles=-1, small_tail=-1),
     dict(mode=E.THRESH_QUANTILE, quantile=0.3, degree_split=2, small_tail=-1),
     # ablation switches: each turns a technique off; the answer must not change
     dict(flags=E.FLAG_NO_GUARDS),
