@@ -50,7 +50,6 @@ constexpr int kGran = 128;             // entries per tile->vertex table step (t
 #define ECL_PAIR_LOG 10
 #endif
 constexpr int kRoundThreads = ECL_ROUND_THREADS;  // threads of a round CTA (one worklist entry each per tile)
-static_assert(2 * kRoundThreads >= kMaxRoundCtas, "seg_load: two segments per thread of a round CTA");
 #ifndef ECL_ROUND_EPT
 #define ECL_ROUND_EPT 1
 #endif
@@ -63,6 +62,9 @@ constexpr int kPairLog = ECL_PAIR_LOG; // parallel-edge table
 constexpr int kPairSlots = 1 << kPairLog;
 constexpr u64 kNoPair = ~0ull;
 constexpr int kSplitAfter = 8;         // find steps before path splitting starts
+#ifndef ECL_L2_HINTS
+#define ECL_L2_HINTS 1                 // evict-first CSR streams, evict-last parent gathers in the scans
+#endif
 constexpr unsigned long long kBarrierTimeoutNs = 5ull * 1000 * 1000 * 1000;
 
 // Entries per thread of the edge-balanced scan for a degree split: rows
@@ -440,6 +442,7 @@ __device__ void scan_produce(const ScanArgs& a, unsigned char* smem, int ntiles)
   const int n = a.nodes, m = a.edges;
   const bool edge_bulk = a.vec_ok != 0;
   const bool idx_bulk = (((uintptr_t)a.nindex) & 15) == 0;
+  const u64 stream_pol = l2_policy_evict_first();  // the CSR is read once per scan
   // Lanes 0..7 read the vertex of each consumer warp's first entry, lane 8
   // the vertex of the next tile's first entry (first_v has one entry per
   // kGran entries), one tile ahead of the copies.
@@ -491,8 +494,13 @@ __device__ void scan_produce(const ScanArgs& a, unsigned char* smem, int ntiles)
       fence_proxy_async_smem();
       mbar_arrive_tx(&full[s], 4u * (unsigned)(2 * bulk_e + bulk_x));
       if (bulk_e) {
-        bulk_g2s(nl, a.nlist + j0, 4u * (unsigned)bulk_e, &full[s]);
-        bulk_g2s(ew, a.eweight + j0, 4u * (unsigned)bulk_e, &full[s]);
+        if (ECL_L2_HINTS) {
+          bulk_g2s_hint(nl, a.nlist + j0, 4u * (unsigned)bulk_e, &full[s], stream_pol);
+          bulk_g2s_hint(ew, a.eweight + j0, 4u * (unsigned)bulk_e, &full[s], stream_pol);
+        } else {
+          bulk_g2s(nl, a.nlist + j0, 4u * (unsigned)bulk_e, &full[s]);
+          bulk_g2s(ew, a.eweight + j0, 4u * (unsigned)bulk_e, &full[s]);
+        }
       }
       if (bulk_x) bulk_g2s(sx, a.nindex + a0, 4u * (unsigned)bulk_x, &full[s]);
     }
@@ -539,6 +547,7 @@ __global__ void __launch_bounds__(kScanThreads, ScanCfg<EPT>::kMinBlocks) k_scan
   for (int q = lane; q < R; q += 32) rmark[q] = 0;
   __syncwarp();
   const int thr = st->threshold;
+  const u64 keep_pol = l2_policy_evict_last();  // parent[] is gathered by every consumer warp
   unsigned* ctr = &st->wl_count[KIND][0];
   unsigned wpos = 0, wend = 0, kept = 0;  // this warp's reserved, unused slots [wpos, wend)
   unsigned idmax = 0;                     // largest neighbour id seen, as unsigned
@@ -653,10 +662,10 @@ __global__ void __launch_bounds__(kScanThreads, ScanCfg<EPT>::kMinBlocks) k_scan
         if (cand & (1u << q)) {
           if (vtx[q] != rv) {
             rv = vtx[q];
-            rrep = __ldg(a.parent + rv);
+            rrep = ECL_L2_HINTS ? ld_cg_hint(a.parent + rv, keep_pol) : __ldg(a.parent + rv);
           }
           vtx[q] = rrep;
-          nrep[q] = __ldg(a.parent + nb[q]);
+          nrep[q] = ECL_L2_HINTS ? ld_cg_hint(a.parent + nb[q], keep_pol) : __ldg(a.parent + nb[q]);
         }
 #pragma unroll
       for (int q = 0; q < EPT; q++)
@@ -796,18 +805,22 @@ __device__ __forceinline__ void seg_set_dense(RoundSmem& s, unsigned count) {
 
 // The list read next is the one the grid's find/min pass just wrote (`nseg`
 // segments, published in the control block before the grid barrier). The
-// whole CTA builds the prefix table: thread t loads segments 2t and 2t + 1
-// (nseg <= kMaxRoundCtas = 2 x the round CTA's threads), one warp scan and
-// one pass over the warp totals give the prefixes. Every thread of the CTA
-// must call this; the caller synchronises the CTA before the table is used.
+// whole CTA builds the prefix table: thread t loads kSegPer consecutive
+// segment counts, one warp scan and one pass over the warp totals give the
+// prefixes. Every thread of the CTA must call this; the caller synchronises
+// the CTA before the table is used.
+constexpr int kSegPer = (kMaxRoundCtas + kRoundThreads - 1) / kRoundThreads;
 __device__ __forceinline__ void seg_load(RoundSmem& s, const DevState* st, int nseg) {
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const int b0 = 2 * t, b1 = 2 * t + 1;
-  const unsigned c0 = b0 < nseg ? __ldcg(&st->seg_cnt[b0]) : 0u;
-  const unsigned c1 = b1 < nseg ? __ldcg(&st->seg_cnt[b1]) : 0u;
-  if (b0 < nseg) s.seg_off[b0] = __ldcg(&st->seg_off[b0]);
-  if (b1 < nseg) s.seg_off[b1] = __ldcg(&st->seg_off[b1]);
-  const unsigned mine = c0 + c1;
+  const int b0 = kSegPer * t;
+  unsigned c[kSegPer], mine = 0;
+#pragma unroll
+  for (int k = 0; k < kSegPer; k++) {
+    const int b = b0 + k;
+    c[k] = b < nseg ? __ldcg(&st->seg_cnt[b]) : 0u;
+    if (b < nseg) s.seg_off[b] = __ldcg(&st->seg_off[b]);
+    mine += c[k];
+  }
   unsigned incl = mine;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -816,12 +829,15 @@ __device__ __forceinline__ void seg_load(RoundSmem& s, const DevState* st, int n
   }
   if (lane == 31) s.rs.warp_off[warp][0] = incl;
   __syncthreads();
-  unsigned before = 0;
-  for (int w = 0; w < warp; w++) before += s.rs.warp_off[w][0];
-  const unsigned excl = before + incl - mine;
-  if (b0 < nseg) s.seg_q[b0] = excl;
-  if (b1 < nseg) s.seg_q[b1] = excl + c0;
-  if (b0 < nseg && nseg <= b1 + 1) s.seg_q[nseg] = excl + mine;  // the thread holding the last segment
+  unsigned q = incl - mine;
+  for (int w = 0; w < warp; w++) q += s.rs.warp_off[w][0];
+#pragma unroll
+  for (int k = 0; k < kSegPer; k++) {
+    const int b = b0 + k;
+    if (b < nseg) s.seg_q[b] = q;
+    q += c[k];
+    if (b == nseg - 1) s.seg_q[nseg] = q;  // the thread holding the last segment
+  }
   if (t == 0) s.seg_n = nseg;
 }
 

@@ -164,6 +164,38 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       : "memory");
 }
 
+// ---- L2 eviction priorities (createpolicy + .L2::cache_hint, sm_80 and
+// later). Streams read once (the CSR in the scans) are marked evict-first so
+// they do not push out the small arrays every thread gathers from (parent[],
+// the min slots), which are marked evict-last where they are read.
+__device__ __forceinline__ u64 l2_policy_evict_first() {
+  u64 p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ u64 l2_policy_evict_last() {
+  u64 p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+// Global -> shared bulk copy as bulk_g2s, with an L2 cache policy.
+__device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, unsigned bytes, u64* bar, u64 policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
+      : "memory");
+}
+
+// 32-bit global load through L2 (no L1 allocation) with an L2 cache policy.
+__device__ __forceinline__ int ld_cg_hint(const int* p, u64 policy) {
+  int v;
+  asm volatile("ld.global.cg.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy));
+  return v;
+}
+
 // Shared memory of one CTA-wide two-counter reservation.
 struct ReserveSmem {
   unsigned warp_off[32][2];
