@@ -182,7 +182,7 @@ def scan_kernel_bytes(st, nodes, edges, entry_bytes=16):
     return b
 
 
-def batch_leg(args, E, torch, dev, rank=0, world=1, dist=None):
+def batch_leg(args, E, torch, dev, rank=0, world=1, dist=None, mode=None):
     """Mixed-family batch (graphs seeded 1000, 1001, ...; sizes log-uniform in
     [1e3, 2e6] vertices; grid / ER deg 8 / RMAT ef 8 / RGG2D deg 3; weights
     U[1, 2^20]): the first `args.batch` graphs of the 4096-graph sequence, solved
@@ -221,7 +221,10 @@ def batch_leg(args, E, torch, dev, rank=0, world=1, dist=None):
     flush = torch.zeros(256 << 20, dtype=torch.uint8, device=dev)
     bc = E.BatchContext(count, int(b.nodes.max()), int(b.edges.max()), 1 << 21)
     stream = torch.cuda.current_stream(dev).cuda_stream
-    best, tune_ms = bc.autotune(b, d_ni, d_nl, d_ew, out.data_ptr())
+    # autotuned around the headline schedule (the learned one serves the
+    # batch's large graphs; the per-CTA small graphs take the heuristic)
+    base = E.make_opts(mode=mode if mode is not None else E.THRESH_HEURISTIC)
+    best, tune_ms = bc.autotune(b, d_ni, d_nl, d_ew, out.data_ptr(), base=base)
     for _ in range(2):
         bc.run(b, d_ni, d_nl, d_ew, out.data_ptr(), opts=best, stream=stream)
     ms = []
@@ -251,6 +254,8 @@ def batch_leg(args, E, torch, dev, rank=0, world=1, dist=None):
            "ms_small": last["ms_small"], "ms_large": last["ms_large"],
            "autotuned": {"batch_small_edges": best.batch_small_edges, "degree_split": best.degree_split,
                          "small_tail": best.small_tail},
+           "schedule": {E.THRESH_LEARNED: "learned (large graphs) / heuristic (per-CTA graphs)"}.get(
+               best.threshold_mode, "heuristic"),
            "generated_on": "device" if on_device else "host", "gen_s": round(gen_s, 1),
            "sample": (f"the whole 4096-graph mixed batch" if count == 4096 else
                       f"first {count} graphs of the 4096-graph mixed batch (seeds 1000..{999 + count})")}
@@ -700,7 +705,7 @@ def main():
     batch = None
     if args.batch > 0:
         # one GPU: the whole batch; several: each rank its shard of the graphs (shard.py)
-        batch = batch_leg(args, E, torch, dev, rank, world, dist if world > 1 else None)
+        batch = batch_leg(args, E, torch, dev, rank, world, dist if world > 1 else None, mode=mode)
 
     grid = None
     if rank == 0 and not args.no_grid and world == 1:

@@ -638,6 +638,7 @@ int check_opts(const mst_opts* o) {
 // Learned threshold/split: extracts graph features on the device and runs the
 // trained MLP, writing DevState::quantile and DevState::learned_split.
 int ecl_learned_prepare(ecl_mst_ctx* c, const ecl_graph* d_graph, cudaStream_t s, void* st);
+int ecl_learned_upload(ecl_mst_ctx* c, cudaStream_t s);
 unsigned ecl_learned_weights_version();
 
 int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, float** feat, void** acc, int** sample,
@@ -1234,6 +1235,9 @@ int batch_enqueue(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST, const 
     key.push_back(o->degree_split);
     key.push_back(o->small_tail);
     key.push_back(o->flags);
+    key.push_back(o->round_min_tiles);
+    key.push_back(o->ctas_per_sm);
+    key.push_back((long long)ecl_learned_weights_version());
     for (int g : large) {
       key.push_back(g);
       key.push_back(b->nindex_off[g]);
@@ -1241,14 +1245,35 @@ int batch_enqueue(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST, const 
       key.push_back(b->nodes[g]);
       key.push_back(b->edges[g]);
     }
+    // The learned schedule runs for the large graphs it serves (as the
+    // single-graph solve: at least kLearnedMinEdges entries, weights loaded),
+    // its feature pass on the engine's side stream beside k_prep; the others
+    // take the reference heuristic.
     mst_opts lo = *o;
-    if (lo.threshold_mode == ECL_THRESH_LEARNED) lo.threshold_mode = ECL_THRESH_HEURISTIC;
+    const bool learned = lo.threshold_mode == ECL_THRESH_LEARNED && ecl_learned_has_weights();
+    if (lo.threshold_mode == ECL_THRESH_LEARNED && !learned) lo.threshold_mode = ECL_THRESH_HEURISTIC;
+    if (learned) {
+      const int r = ecl_learned_upload(c->big, s);  // before any capture
+      if (r) return r;
+    }
     auto enqueue_large = [&](cudaStream_t q) -> int {
       for (int g : large) {
         ecl_graph dg = {b->nodes[g], b->edges[g], b->nindex + b->nindex_off[g], b->nlist + b->edge_off[g],
                         b->eweight + b->edge_off[g]};
         ECL_CUDA_TRY(cudaMemsetAsync(c->big->st, 0, sizeof(DevState), q));
-        int r = enqueue_solve(c->big, &dg, d_inMST + b->edge_off[g], &lo, q, false);
+        mst_opts go = lo;
+        cudaEvent_t join = nullptr;
+        if (learned && dg.edges >= kLearnedMinEdges) {
+          ECL_CUDA_TRY(cudaEventRecord(c->big->fork, q));
+          ECL_CUDA_TRY(cudaStreamWaitEvent(c->big->side, c->big->fork, 0));
+          int r = ecl_learned_prepare(c->big, &dg, c->big->side, c->big->st);
+          if (r) return r;
+          ECL_CUDA_TRY(cudaEventRecord(c->big->join, c->big->side));
+          join = c->big->join;
+        } else if (go.threshold_mode == ECL_THRESH_LEARNED) {
+          go.threshold_mode = ECL_THRESH_HEURISTIC;
+        }
+        int r = enqueue_solve(c->big, &dg, d_inMST + b->edge_off[g], &go, q, false, join);
         if (r) return r;
         k_or_error<<<1, 1, 0, q>>>(c->big->st, c->st);
         ECL_CUDA_TRY(cudaGetLastError());

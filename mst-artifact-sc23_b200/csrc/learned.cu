@@ -363,6 +363,27 @@ unsigned ecl_learned_weights_version() {
 // quantile and split into the solve's control block. Returns
 // ECL_ERR_UNSUPPORTED when no weights are loaded (the caller then falls back
 // to the reference heuristic).
+// Upload the loaded weights to the context's parameter buffer if they
+// changed since its last upload (synchronous: call it outside any stream
+// capture before capturing learned solves).
+int ecl_learned_upload(ecl_mst_ctx* c, cudaStream_t s) {
+  float *d_params, *d_feat;
+  void* d_acc;
+  int* d_sample;
+  unsigned* version;
+  int sms = 0;
+  int r = ecl_ctx_learned_buffers(c, &d_params, &d_feat, &d_acc, &d_sample, &version, &sms);
+  if (r) return r;
+  std::lock_guard<std::mutex> lock(g_w_mu);
+  if (g_weights.empty()) return ECL_ERR_UNSUPPORTED;
+  if (*version != g_w_version) {
+    ML_TRY(cudaMemcpyAsync(d_params, g_weights.data(), kParams * sizeof(float), cudaMemcpyHostToDevice, s));
+    ML_TRY(cudaStreamSynchronize(s));
+    *version = g_w_version;
+  }
+  return ECL_OK;
+}
+
 int ecl_learned_prepare(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s, void* st) {
   float *d_params, *d_feat;
   void* d_acc;

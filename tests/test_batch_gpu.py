@@ -87,3 +87,16 @@ def test_batch_autotune_keeps_the_answer():
         t, f = E.heuristic_threshold(g) if g.edges else (2**31 - 1, 0)
         assert np.array_equal(b.slice(got, gi), O.oracle_mst(g.nindex, g.nlist, g.eweight, t, f)[0])
     bc.close()
+
+
+def test_batch_learned_schedule_on_large_graphs():
+    """Large graphs of a batch (beyond the per-CTA cutoff, at least 2^20 CSR
+    entries) take the learned schedule, feature pass on a side stream inside
+    the captured launch sequence; every graph keeps the oracle's forest."""
+    if not E.learned_load_default():
+        pytest.skip("no trained weights shipped")
+    graphs = _mixed_graphs(4000, 12) + [
+        E.gen_rmat(17, 16, 0.57, 0.19, 0.19, 4101, 1 << 20), E.gen_er(200_000, 12, 4102, 1 << 20),
+        E.gen_grid(700, 700, 4103, 1 << 20), E.gen_rgg2d(400_000, 3, 4104, 1 << 20)]
+    sts = _run(graphs, 1 << 16, [E.make_opts(mode=E.THRESH_LEARNED)])
+    assert all(s["graphs_large"] >= 4 and s["status"] == 0 for s in sts)
