@@ -399,9 +399,10 @@ int ecl_mst_run_batch_device(ecl_batch_ctx* ctx, const ecl_batch* batch,
                              ecl_batch_stats* stats);
 
 /* Autotuner: times candidate schedules (per-CTA cutoff, scan entries per
- * thread, single-CTA tail size) on the batch and writes the fastest into
- * *best (a copy of *base with those fields set). The answer is the same for
- * every candidate; only the time differs. */
+ * thread and, when *base asks for the learned schedule, learned against the
+ * reference heuristic for the large graphs) on the batch and writes the
+ * fastest into *best (a copy of *base with those fields set). The answer is
+ * the same for every candidate; only the time differs. */
 int ecl_batch_autotune(ecl_batch_ctx* ctx, const ecl_batch* batch, uint8_t* d_inMST,
                        const mst_opts* base, mst_opts* best, float* best_ms);
 

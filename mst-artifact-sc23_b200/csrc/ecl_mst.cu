@@ -1366,21 +1366,24 @@ extern "C" int ecl_batch_autotune(ecl_batch_ctx* c, const ecl_batch* b, uint8_t*
   mst_opts best_o = o0;
   const int cutoffs[] = {c->cap / 8, c->cap / 4, c->cap / 2, c->cap};
   const int splits[] = {8, 16};
-  const int tails[] = {4096, 16384};
-  for (int cut : cutoffs) {
-    if (cut < 1) continue;
-    for (int sp : splits) {
-      for (int tl : tails) {
+  // The learned schedule (large graphs only) is kept only where it beats the
+  // reference heuristic on this batch.
+  const int modes[] = {o0.threshold_mode, ECL_THRESH_HEURISTIC};
+  const int nmodes = o0.threshold_mode == ECL_THRESH_LEARNED ? 2 : 1;
+  for (int mi = 0; mi < nmodes; mi++) {
+    for (int cut : cutoffs) {
+      if (cut < 1) continue;
+      for (int sp : splits) {
         mst_opts o = o0;
+        o.threshold_mode = modes[mi];
         o.batch_small_edges = cut;
         o.degree_split = sp;
-        o.small_tail = tl;
         float t = 0.f;
-        for (int rep = 0; rep < 3; rep++) {
+        for (int rep = 0; rep < 2; rep++) {
           ecl_batch_stats bs;
           int st = ecl_mst_run_batch_device(c, b, d_inMST, &o, nullptr, &bs);
           if (st) return st;
-          if (rep > 0) t += bs.ms_total;  // first run warms up (and captures)
+          if (rep > 0) t += bs.ms_total;  // the first run warms up (and captures)
         }
         if (t < best_t) {
           best_t = t;
@@ -1390,6 +1393,6 @@ extern "C" int ecl_batch_autotune(ecl_batch_ctx* c, const ecl_batch* b, uint8_t*
     }
   }
   *best = best_o;
-  if (best_ms) *best_ms = best_t / 2;
+  if (best_ms) *best_ms = best_t;
   return ECL_OK;
 }
