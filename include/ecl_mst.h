@@ -309,6 +309,22 @@ void ecl_mst_ctx_destroy(ecl_mst_ctx* ctx);
 int ecl_mst_ctx_run_host(ecl_mst_ctx* ctx, const ecl_graph* g, uint8_t* inMST,
                          const mst_opts* opts, ecl_mst_stats* stats);
 
+/* Pipelined host-buffer solves, for a stream of graphs: each call enqueues
+ * the copy in of g's arrays, the solve and the copy back of inMST, and
+ * returns; ecl_mst_ctx_wait waits for every call since the last wait and
+ * reports their device errors. Consecutive calls overlap: a graph's copy in
+ * runs beside the previous graph's solve and copy back (two device buffer
+ * sets used in turn, a copy-in and a copy-out stream beside the context's).
+ * g's arrays and inMST must stay valid until the wait, and pinned host
+ * memory (ecl_host_alloc_pinned) keeps the copies asynchronous. Call
+ * ecl_mst_ctx_wait before any other solve on the context. An input with
+ * more one-direction entries than edges/2 is solved again inside the wait,
+ * with grown worklists. No counterpart in the reference, which solves one
+ * graph per process run. */
+int ecl_mst_ctx_run_host_async(ecl_mst_ctx* ctx, const ecl_graph* g,
+                               uint8_t* inMST, const mst_opts* opts);
+int ecl_mst_ctx_wait(ecl_mst_ctx* ctx);
+
 /* Device-resident solve: d_graph holds DEVICE pointers, d_inMST is a device
  * buffer of edges bytes. Enqueued on `stream` (cudaStream_t, NULL = the
  * context's stream); returns after enqueueing unless stats != NULL, in which

@@ -62,6 +62,29 @@ struct ecl_mst_ctx {
   mst_opts pend_opts = {};
   cudaStream_t pend_stream = nullptr;
   bool resolved = false;  // the last ecl_mst_ctx_sync repeated the solve
+  // pipelined host-buffer solves (ecl_mst_ctx_run_host_async): two device
+  // buffer sets used in turn (set 0 is the one run_host uses), a copy-in and a
+  // copy-out stream, the events that order them, a sticky device error word
+  // and the calls since the last ecl_mst_ctx_wait (repeated after a
+  // worklist overflow)
+  struct HostSet {
+    int* nindex = nullptr;
+    int* nlist = nullptr;
+    int* eweight = nullptr;
+    unsigned char* inMST = nullptr;
+    cudaEvent_t in_done = nullptr, solved = nullptr, out_done = nullptr;
+    bool used = false;
+  };
+  HostSet hs[2];
+  cudaStream_t cin = nullptr, cout = nullptr;
+  unsigned async_seq = 0;
+  unsigned* sticky = nullptr;
+  struct AsyncCall {
+    ecl_graph g;
+    uint8_t* out;
+    mst_opts opts;
+  };
+  std::vector<AsyncCall> async_calls;
   int* slist = nullptr;    // ECL_FLAG_NO_TUPLES: vertex of every CSR entry (allocated on first use)
   int vertex_grid = 0;     // ECL_FLAG_NO_EDGE_BASED: cooperative grid of the vertex-centric rounds
   int* first_v = nullptr;  // tile -> vertex table of the edge-balanced scans
@@ -305,6 +328,18 @@ extern "C" void ecl_mst_ctx_destroy(ecl_mst_ctx* c) {
   cudaFree(c->d_nlist);
   cudaFree(c->d_eweight);
   cudaFree(c->d_inMST);
+  if (c->cin) cudaStreamSynchronize(c->cin);
+  if (c->cout) cudaStreamSynchronize(c->cout);
+  cudaFree(c->hs[1].nindex);
+  cudaFree(c->hs[1].nlist);
+  cudaFree(c->hs[1].eweight);
+  cudaFree(c->hs[1].inMST);
+  cudaFree(c->sticky);
+  for (auto& h : c->hs)
+    for (cudaEvent_t e : {h.in_done, h.solved, h.out_done})
+      if (e) cudaEventDestroy(e);
+  if (c->cin) cudaStreamDestroy(c->cin);
+  if (c->cout) cudaStreamDestroy(c->cout);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->side) cudaStreamSynchronize(c->side);
@@ -808,18 +843,27 @@ extern "C" int ecl_mst_run_device(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d
   return st;
 }
 
+namespace {
+
+// Device CSR and inMST buffers for host-buffer solves, allocated on first use.
+int host_buffers(ecl_mst_ctx* c, int** ni, int** nl, int** ew, unsigned char** out) {
+  if (*ni) return ECL_OK;
+  const size_t nb = ((size_t)c->max_nodes + 1) * 4, eb = (size_t)std::max<int64_t>(c->max_edges, 1) * 4;
+  ECL_CUDA_TRY(cudaMalloc(ni, nb));
+  ECL_CUDA_TRY(cudaMalloc(nl, eb));
+  ECL_CUDA_TRY(cudaMalloc(ew, eb));
+  ECL_CUDA_TRY(cudaMalloc(out, eb / 4));
+  return ECL_OK;
+}
+
+}  // namespace
+
 extern "C" int ecl_mst_ctx_run_host(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* inMST,
                                     const mst_opts* opts, ecl_mst_stats* stats) {
   int st = check_graph_args(c, g, inMST);
   if (st) return st;
   ECL_CUDA_TRY(cudaSetDevice(c->device));
-  const size_t nb = ((size_t)c->max_nodes + 1) * 4, eb = (size_t)std::max<int64_t>(c->max_edges, 1) * 4;
-  if (!c->d_nindex) {
-    ECL_CUDA_TRY(cudaMalloc(&c->d_nindex, nb));
-    ECL_CUDA_TRY(cudaMalloc(&c->d_nlist, eb));
-    ECL_CUDA_TRY(cudaMalloc(&c->d_eweight, eb));
-    ECL_CUDA_TRY(cudaMalloc(&c->d_inMST, eb / 4));
-  }
+  if ((st = host_buffers(c, &c->d_nindex, &c->d_nlist, &c->d_eweight, &c->d_inMST))) return st;
   const int n = g->nodes, m = g->edges;
   ECL_CUDA_TRY(cudaMemcpyAsync(c->d_nindex, g->nindex, ((size_t)n + 1) * 4, cudaMemcpyHostToDevice, c->stream));
   if (m > 0) {
@@ -847,6 +891,100 @@ extern "C" int ecl_mst_ctx_run_host(ecl_mst_ctx* c, const ecl_graph* g, uint8_t*
     stats->forest_weight = fw;
   }
   return ECL_OK;
+}
+
+namespace {
+
+__global__ void k_sticky_or(const DevState* st, unsigned* sticky) {
+  const unsigned e = ld_volatile(&st->error);
+  if (e) atomicOr(sticky, e);
+}
+
+// Streams, events, the second buffer set and the sticky error word of the
+// pipelined solves, created on first use.
+int async_setup(ecl_mst_ctx* c) {
+  if (c->cin) return ECL_OK;
+  int st;
+  if ((st = host_buffers(c, &c->d_nindex, &c->d_nlist, &c->d_eweight, &c->d_inMST))) return st;
+  c->hs[0].nindex = c->d_nindex;
+  c->hs[0].nlist = c->d_nlist;
+  c->hs[0].eweight = c->d_eweight;
+  c->hs[0].inMST = c->d_inMST;
+  if ((st = host_buffers(c, &c->hs[1].nindex, &c->hs[1].nlist, &c->hs[1].eweight, &c->hs[1].inMST))) return st;
+  for (auto& h : c->hs)
+    for (cudaEvent_t* e : {&h.in_done, &h.solved, &h.out_done})
+      ECL_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  ECL_CUDA_TRY(cudaMalloc(&c->sticky, sizeof(unsigned)));
+  ECL_CUDA_TRY(cudaMemset(c->sticky, 0, sizeof(unsigned)));
+  ECL_CUDA_TRY(cudaStreamCreateWithFlags(&c->cout, cudaStreamNonBlocking));
+  ECL_CUDA_TRY(cudaStreamCreateWithFlags(&c->cin, cudaStreamNonBlocking));
+  return ECL_OK;
+}
+
+}  // namespace
+
+extern "C" int ecl_mst_ctx_run_host_async(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* inMST,
+                                          const mst_opts* opts) {
+  int st = check_graph_args(c, g, inMST);
+  if (st) return st;
+  ECL_CUDA_TRY(cudaSetDevice(c->device));
+  if ((st = async_setup(c))) return st;
+  auto& h = c->hs[c->async_seq++ & 1];
+  const int n = g->nodes, m = g->edges;
+  // copy in, once the solve that last read this set's CSR has finished
+  if (h.used) ECL_CUDA_TRY(cudaStreamWaitEvent(c->cin, h.solved, 0));
+  ECL_CUDA_TRY(cudaMemcpyAsync(h.nindex, g->nindex, ((size_t)n + 1) * 4, cudaMemcpyHostToDevice, c->cin));
+  if (m > 0) {
+    ECL_CUDA_TRY(cudaMemcpyAsync(h.nlist, g->nlist, (size_t)m * 4, cudaMemcpyHostToDevice, c->cin));
+    ECL_CUDA_TRY(cudaMemcpyAsync(h.eweight, g->eweight, (size_t)m * 4, cudaMemcpyHostToDevice, c->cin));
+  }
+  ECL_CUDA_TRY(cudaEventRecord(h.in_done, c->cin));
+  // solve on the context's stream once the inputs are in and the set's
+  // previous inMST has been copied out; its device errors accumulate
+  ECL_CUDA_TRY(cudaStreamWaitEvent(c->stream, h.in_done, 0));
+  if (h.used) ECL_CUDA_TRY(cudaStreamWaitEvent(c->stream, h.out_done, 0));
+  ecl_graph dg = {n, m, h.nindex, h.nlist, h.eweight};
+  if ((st = run_device_once(c, &dg, h.inMST, opts, c->stream, nullptr))) return st;
+  k_sticky_or<<<1, 1, 0, c->stream>>>(c->st, c->sticky);
+  ECL_CUDA_TRY(cudaGetLastError());
+  ECL_CUDA_TRY(cudaEventRecord(h.solved, c->stream));
+  // copy out beside the next graph's copy in and solve
+  ECL_CUDA_TRY(cudaStreamWaitEvent(c->cout, h.solved, 0));
+  if (m > 0) ECL_CUDA_TRY(cudaMemcpyAsync(inMST, h.inMST, (size_t)m, cudaMemcpyDeviceToHost, c->cout));
+  ECL_CUDA_TRY(cudaEventRecord(h.out_done, c->cout));
+  h.used = true;
+  ecl_mst_ctx::AsyncCall call;
+  call.g = *g;
+  call.out = inMST;
+  if (opts) call.opts = *opts;
+  else ecl_default_opts(&call.opts);
+  c->async_calls.push_back(call);
+  c->pending = false;
+  return ECL_OK;
+}
+
+extern "C" int ecl_mst_ctx_wait(ecl_mst_ctx* c) {
+  if (!c) return ECL_ERR_INVALID_ARG;
+  ECL_CUDA_TRY(cudaSetDevice(c->device));
+  if (!c->cin) return ECL_OK;
+  ECL_CUDA_TRY(cudaStreamSynchronize(c->cin));
+  ECL_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  ECL_CUDA_TRY(cudaStreamSynchronize(c->cout));
+  unsigned err = 0;
+  ECL_CUDA_TRY(cudaMemcpy(&err, c->sticky, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  ECL_CUDA_TRY(cudaMemset(c->sticky, 0, sizeof(unsigned)));
+  std::vector<ecl_mst_ctx::AsyncCall> calls;
+  calls.swap(c->async_calls);
+  if ((err & kErrOverflow) && !c->wl_full) {
+    // an input had more one-direction entries than half its CSR entries:
+    // grow the worklists and solve the calls since the last wait again
+    int st = grow_worklists(c);
+    if (st) return st;
+    for (auto& call : calls)
+      if ((st = ecl_mst_ctx_run_host(c, &call.g, call.out, &call.opts, nullptr))) return st;
+    return ECL_OK;
+  }
+  return device_error_status(err);
 }
 
 extern "C" int ecl_mst_run(const ecl_graph* g, uint8_t* inMST, const mst_opts* opts,

@@ -130,6 +130,8 @@ def load():
         "ecl_mst_run_device_noalloc": (c_int, [G, c_void_p, POINTER(MstOpts), c_void_p]),
         "ecl_mst_ctx_stream": (c_void_p, [c_void_p]),
         "ecl_mst_ctx_l2_reset": (c_int, [c_void_p]),
+        "ecl_mst_ctx_run_host_async": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+        "ecl_mst_ctx_wait": (c_int, [c_void_p]),
         "ecl_host_alloc_pinned": (c_int, [ctypes.c_size_t, POINTER(c_void_p)]),
         "ecl_host_free_pinned": (None, [c_void_p]),
         "ecl_batch_ctx_create": (c_int, [c_int, c_int32, c_int64, c_int64, c_int32, POINTER(c_void_p)]),
@@ -485,6 +487,7 @@ class Context:
         h = c_void_p()
         _check(self._lib.ecl_mst_ctx_create(device, max_nodes, max_edges, ctypes.byref(h)), "ctx_create")
         self.handle = h
+        self._inflight = []  # arrays of run_host_async calls not yet waited for
 
     def close(self):
         if self.handle:
@@ -517,6 +520,27 @@ class Context:
                                               None if opts is None else ctypes.byref(opts),
                                               None if st is None else ctypes.byref(st)), "ctx_run_host")
         return out[: g.edges], (st.as_dict() if st is not None else None)
+
+    def run_host_async(self, g, opts=None, out=None):
+        """Enqueue a host-buffer solve (copy in, solve, copy back) that overlaps
+        the previous one; the result lands in `out` by the next wait(). The
+        arrays are kept referenced until then."""
+        if out is None:
+            out = np.zeros(max(g.edges, 1), np.uint8)
+        gs = g.struct()
+        keep = (g, out, gs, opts)
+        _check(self._lib.ecl_mst_ctx_run_host_async(self.handle, ctypes.byref(gs), _ptr(out),
+                                                    None if opts is None else ctypes.byref(opts)),
+               "ctx_run_host_async")
+        self._inflight.append(keep)
+        return out[: g.edges]
+
+    def wait(self):
+        """Wait for every run_host_async call since the last wait."""
+        try:
+            _check(self._lib.ecl_mst_ctx_wait(self.handle), "ctx_wait")
+        finally:
+            self._inflight = []
 
     def run_device(self, nodes, edges, d_nindex, d_nlist, d_eweight, d_inMST, opts=None, stream=None,
                    stats=False):

@@ -388,3 +388,28 @@ def test_one_direction_input_grows_the_worklists(k):
                          stream=torch.cuda.current_stream().cuda_stream, stats=stats)
             c.sync()
             assert np.array_equal(out.cpu().numpy(), want), stats
+
+
+def test_pipelined_host_solves_match_the_oracle():
+    """run_host_async overlaps each graph's copy in with the previous solve
+    and copy back; after wait() every output is the oracle's, including an
+    input whose one-direction entries overflow the half-size worklists
+    (solved again inside the wait)."""
+    import torch
+    graphs = [E.gen_rmat(16, 16, 0.57, 0.19, 0.19, 21, 1 << 24), E.gen_grid(300, 300, 22, 1000),
+              _forward_only(1 << 20, 3, 23), E.gen_er(50_000, 10, 24, 1 << 20), E.gen_rmat(15, 8, 0.57, 0.19, 0.19, 25, 99)]
+    wants = []
+    for g in graphs:
+        t, f = E.heuristic_threshold(g)
+        wants.append(O.oracle_mst(g.nindex, g.nlist, g.eweight, t, f)[0])
+    with E.Context(max(g.nodes for g in graphs), max(g.edges for g in graphs)) as c:
+        for rep in range(2):
+            outs = []
+            for g in graphs:
+                pinned = [torch.from_numpy(a).pin_memory().numpy() for a in (g.nindex, g.nlist, g.eweight)]
+                hg = E.Graph(*pinned)
+                outs.append(c.run_host_async(hg, E.make_opts(mode=E.THRESH_LEARNED if rep else E.THRESH_HEURISTIC),
+                                             out=torch.full((g.edges,), 7, dtype=torch.uint8).pin_memory().numpy()))
+            c.wait()
+            for i, (got, want) in enumerate(zip(outs, wants)):
+                assert np.array_equal(got, want), (rep, i)
