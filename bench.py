@@ -612,8 +612,12 @@ def main():
 
     if args.profile:
         if rank == 0:
+            # the algorithmic bytes of this workload's kernels (to scale a small
+            # capture's DRAM traffic to a larger workload)
             print(json.dumps({"workload": args.workload, "ms_per_step": ms_step, "value": value,
-                              "rounds": last["rounds"], "forest_weight": fw}), flush=True)
+                              "rounds": last["rounds"], "forest_weight": fw,
+                              "round_bytes": round_kernel_bytes(last, g.nodes, atomics=st_atom["atomics"]),
+                              "scan_bytes": scan_kernel_bytes(last, g.nodes, g.edges)}), flush=True)
         ctx.close()
         return
 
