@@ -37,11 +37,14 @@ namespace ecl {
 
 constexpr int kThreads = 512;          // threads of the prep, flatten and batch kernels
 constexpr int kGran = 128;             // entries per tile->vertex table step (the smallest scan warp range)
+// Round CTAs of 1024 threads, two per SM (measured on RMAT-22: 2.4 % faster
+// with the learned schedule and 4.6 % with the heuristic one than 512 x 4;
+// 256 x 8 was 11-15 % slower)
 #ifndef ECL_ROUND_THREADS
-#define ECL_ROUND_THREADS 512
+#define ECL_ROUND_THREADS 1024
 #endif
 #ifndef ECL_ROUND_MIN_BLOCKS
-#define ECL_ROUND_MIN_BLOCKS 4
+#define ECL_ROUND_MIN_BLOCKS 2
 #endif
 #ifndef ECL_FIND_LOG
 #define ECL_FIND_LOG 10
