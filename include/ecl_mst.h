@@ -187,7 +187,9 @@ int ecl_heuristic_threshold(const ecl_graph* g, int32_t* threshold,
 
 /* --------------------------------------------------------------- options */
 enum {
-  ECL_FLAG_L2_PERSIST = 1 << 0, /* L2 access-policy window on parent/min slots   */
+  ECL_FLAG_L2_PERSIST = 1 << 0, /* L2 access-policy window on parent/min slots
+                                   (opt-in: measured 6 % slower on RMAT-22, the
+                                   set-aside takes L2 from the heavy scan)      */
   ECL_FLAG_STATS = 1 << 1,      /* count guarded atomics (slower; off in timing) */
   ECL_FLAG_NO_SMALL_TAIL = 1 << 2, /* keep every round grid-wide (ablation)     */
   /* Ablation switches: each turns one technique of the round kernel off, to
