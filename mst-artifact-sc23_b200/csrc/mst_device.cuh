@@ -867,32 +867,6 @@ __device__ __forceinline__ unsigned seg_at(const RoundSmem& s, unsigned i) {
   return s.seg_off[lo] + (i - s.seg_q[lo]);
 }
 
-// seg_at for the 32 consecutive logical indices of a warp (every lane calls
-// it): lanes 0 and 31 locate their segments, and only a warp that straddles
-// segments searches again, per lane, between the two. One search per warp
-// instead of one per lane in the common case.
-#ifndef ECL_SEG_WARP
-#define ECL_SEG_WARP 1
-#endif
-__device__ __forceinline__ unsigned seg_at_warp(const RoundSmem& s, unsigned i) {
-  const int nseg = s.seg_n;
-  if (nseg == 1) return s.seg_off[0] + i;
-  if (!ECL_SEG_WARP) return seg_at(s, i);
-  const int lane = threadIdx.x & 31;
-  auto search = [&](int lo, int hi) {  // largest b in [lo, hi) with seg_q[b] <= i
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (s.seg_q[mid] <= i) lo = mid;
-      else hi = mid;
-    }
-    return lo;
-  };
-  int b = (lane == 0 || lane == 31) ? search(0, nseg) : 0;
-  const int b0 = __shfl_sync(0xffffffffu, b, 0), b1 = __shfl_sync(0xffffffffu, b, 31);
-  b = b0 == b1 ? b0 : search(b0, b1 + 1);
-  return s.seg_off[b] + (i - s.seg_q[b]);
-}
-
 // First output position of tile share `b` of a pass over W logical entries
 // in tiles of `tile`, shares strided by `stride`: the logical entries of the
 // tiles of all shares before b (the last tile may be partial).
@@ -1198,8 +1172,7 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
     for (int k = 0; k < kEPT; k++) {
       const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
       in_range[k] = idx < W;
-      const unsigned pos = seg_at_warp(s, idx);  // every lane: warp-wide shuffles inside
-      e[k] = in_range[k] ? load_entry(a, in, pos) : make_int4(0, 0, 0, 0);
+      e[k] = in_range[k] ? load_entry(a, in, seg_at(s, idx)) : make_int4(0, 0, 0, 0);
       if (e[k].x < 0) in_range[k] = false;  // null entry (unused scan slot)
     }
     int4 orig[kEPT];
@@ -1296,8 +1269,7 @@ __device__ __forceinline__ void round_mark(const RoundArgs& a, const int4* wl, u
     for (int k = 0; k < kEPT; k++) {
       const unsigned idx = t * tile + k * blockDim.x + threadIdx.x;
       in_range[k] = idx < W;
-      const unsigned pos = seg_at_warp(s, idx);  // every lane: warp-wide shuffles inside
-      e[k] = in_range[k] ? load_entry(a, wl, pos) : make_int4(0, 0, 0, 0);
+      e[k] = in_range[k] ? load_entry(a, wl, seg_at(s, idx)) : make_int4(0, 0, 0, 0);
       if (e[k].x < 0) in_range[k] = false;  // null entry (unused scan slot)
     }
     if (keep_ends) {
