@@ -678,12 +678,6 @@ __global__ void __launch_bounds__(kScanThreads, ScanCfg<EPT>::kMinBlocks) k_scan
       for (int q = 0; q < EPT; q++)
         if (vtx[q] == nrep[q]) cand &= ~(1u << q);
     }
-    if (KIND == kLight) {  // a negative light weight rules out ending the light phase early
-      bool neg = false;
-#pragma unroll
-      for (int q = 0; q < EPT; q++) neg |= ((cand >> q) & 1u) && w[q] < 0;
-      if (__any_sync(0xffffffffu, neg) && lane == 0) st->neg_light = 1;
-    }
     const unsigned cnt = __popc(cand);
     // warp reservation: slots from this warp's chunk, then a fresh chunk
     unsigned incl = cnt;
@@ -1393,7 +1387,7 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
     // its mark pass: the heavy phase takes the light entries still between
     // light trees (the heavy scan keeps them). Uniform: every CTA reads the
     // same W and W2.
-    const bool cut = ph == 0 && a.cut && st->filtered && !st->neg_light && !fresh && !ndd &&
+    const bool cut = ph == 0 && a.cut && st->filtered && !fresh && !ndd &&
                      (unsigned long long)W2 * 1024ull >= (unsigned long long)a.cut * W;
     // the list the mark pass and the next round read: the scan's list (round
     // 0), the tail CTA's single segment, or the grid's per-CTA segments

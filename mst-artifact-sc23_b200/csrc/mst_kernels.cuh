@@ -41,9 +41,6 @@ struct DevState {
   unsigned pad;
   int light_cut;       // 1 = the light phase stopped early: the heavy scan also keeps
                        // light entries between light trees
-  int neg_light;       // 1 = the light scan kept a negative weight: light keys (weights
-                       // ordered as uint32) need not sort below the heavy ones, so the
-                       // light phase must run to the end
   float quantile;      // learned / quantile modes: filter quantile in [0,1]
   int learned_split;   // learned mode: predicted degree split
   u64 atomics;         // guarded atomicMin issued (stats mode)
