@@ -256,13 +256,7 @@ typedef struct mst_opts {
                           /* CSR entries (and fitting the per-CTA scratch) are */
                           /* solved one per CTA by the persistent kernel;      */
                           /* 0 = the context's per-CTA capacity                */
-  int32_t light_cut;      /* the light phase stops after a round that keeps at  */
-                          /* least light_cut/1024 of its entries, and the heavy */
-                          /* phase takes the light entries still between light */
-                          /* trees with the heavy ones (same forest; the       */
-                          /* stalled tail of light rounds is skipped);         */
-                          /* 0 = default, < 0 = run the light phase to the end */
-  int32_t reserved[6];
+  int32_t reserved[7];
 } mst_opts;
 
 /* Fill *opts with the defaults (heuristic threshold, reference semantics). */

@@ -22,11 +22,6 @@ namespace {
 constexpr int kDefaultSplit = 8;
 constexpr unsigned kDefaultSmallTail = 4096;
 constexpr int kDefaultMinTiles = 1;  // round CTAs kept: one per tile of the round's worklist
-// light phase cut: a round keeping >= this many 1024ths of its entries ends it
-#ifndef ECL_LIGHT_CUT
-#define ECL_LIGHT_CUT 0
-#endif
-constexpr unsigned kDefaultLightCut = ECL_LIGHT_CUT;
 constexpr int64_t kWlSlack = 1 << 19;  // worklist slots beyond `edges` (scan chunk tails)
 constexpr int kLearnedMinEdges = 1 << 20;
 }  // namespace
@@ -553,9 +548,6 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   // each round, which one CTA of a small tail would do alone
   if (ra.abl & kAblKeepEnds) ra.small_tail = 0;
   ra.min_tiles = o->round_min_tiles < 0 ? 0 : (o->round_min_tiles == 0 ? kDefaultMinTiles : o->round_min_tiles);
-  // the ablations of the reference's structure keep its phase structure
-  ra.cut = (o->light_cut < 0 || (ra.abl & kAblKeepEnds)) ? 0u
-                                                          : (o->light_cut == 0 ? kDefaultLightCut : (unsigned)o->light_cut);
   int rmax = c->round_grid;
   if (o->ctas_per_sm > 0) rmax = std::min(rmax, o->ctas_per_sm * c->sm_count);
   const int rgrid = std::max(1, std::min(rmax, (m / 2 + kRoundThreads - 1) / kRoundThreads + 1));
@@ -672,7 +664,6 @@ int check_opts(const mst_opts* o) {
     return ECL_ERR_INVALID_ARG;
   if (o->degree_split < 0 || o->degree_split > (1 << 20)) return ECL_ERR_INVALID_ARG;
   if (o->ctas_per_sm < 0) return ECL_ERR_INVALID_ARG;
-  if (o->light_cut > 1024) return ECL_ERR_INVALID_ARG;
   if (o->threshold_mode == ECL_THRESH_QUANTILE && !(o->quantile >= 0.0f)) return ECL_ERR_INVALID_ARG;
   return ECL_OK;
 }
@@ -762,8 +753,8 @@ int run_device_once(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d_inMST, const 
   const std::vector<long long> key = {
       g->nodes, g->edges, (long long)(uintptr_t)g->nindex, (long long)(uintptr_t)g->nlist,
       (long long)(uintptr_t)g->eweight, (long long)(uintptr_t)d_inMST, o.threshold_mode, o.threshold,
-      (long long)*(const int*)&qbits, o.degree_split, o.small_tail, o.flags, o.round_min_tiles, o.ctas_per_sm,
-      o.light_cut, (long long)(uintptr_t)c->wl[0], (long long)ecl_learned_weights_version()};
+      (long long)*(const int*)&qbits, o.degree_split, o.small_tail, o.flags,
+      (long long)ecl_learned_weights_version()};
   const bool graph_ok = !(o.flags & ECL_FLAG_NO_GRAPH);
   bool replayed = false;
   auto replay = [&]() -> int {
@@ -1384,7 +1375,6 @@ int batch_enqueue(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST, const 
     key.push_back(o->flags);
     key.push_back(o->round_min_tiles);
     key.push_back(o->ctas_per_sm);
-    key.push_back(o->light_cut);
     key.push_back((long long)ecl_learned_weights_version());
     for (int g : large) {
       key.push_back(g);

@@ -125,7 +125,6 @@ struct RoundArgs {
   int count_atomics;
   unsigned abl;  // kAbl* bits: techniques switched off to measure what they buy
   int min_tiles;  // keep one CTA per this many tiles of a round (0 = every CTA)
-  unsigned cut;   // light phase: stop after a round keeping >= cut/1024 of its entries (0 = never)
   // kAblNoTuples: the CSR and the vertex of every entry
   const int* nlist;
   const int* eweight;
@@ -551,9 +550,6 @@ __global__ void __launch_bounds__(kScanThreads, ScanCfg<EPT>::kMinBlocks) k_scan
   for (int q = lane; q < R; q += 32) rmark[q] = 0;
   __syncwarp();
   const int thr = st->threshold;
-  // a light phase stopped early leaves light entries between light trees to
-  // the heavy phase: the heavy scan keeps every entry whose trees differ
-  const bool light_cut = KIND == kHeavy && st->light_cut != 0;
   const u64 keep_pol = l2_policy_evict_last();  // parent[] is gathered by every consumer warp
   unsigned* ctr = &st->wl_count[KIND][0];
   unsigned wpos = 0, wend = 0, kept = 0;  // this warp's reserved, unused slots [wpos, wend)
@@ -655,7 +651,7 @@ __global__ void __launch_bounds__(kScanThreads, ScanCfg<EPT>::kMinBlocks) k_scan
       const int v = v_lo + vi[q];
       if (q < lim) idmax = max(idmax, (unsigned)nb[q]);
       const bool pass = q < lim && (unsigned)nb[q] - (unsigned)v - 1u < (unsigned)(n - v - 1) &&
-                        (KIND == kLight ? w[q] <= thr : (w[q] > thr || light_cut));
+                        (KIND == kLight ? w[q] <= thr : w[q] > thr);
       cand |= (unsigned)pass << q;
       vtx[q] = v;
       nrep[q] = nb[q];
@@ -1383,12 +1379,6 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
     const unsigned W2 = min(ld_volatile(&st->wl_count[ph][r + 1]), a.wl_cap);
     r++;
     if (W2 == 0) break;
-    // A light round that barely shrank its list ends the light phase after
-    // its mark pass: the heavy phase takes the light entries still between
-    // light trees (the heavy scan keeps them). Uniform: every CTA reads the
-    // same W and W2.
-    const bool cut = ph == 0 && a.cut && st->filtered && !fresh && !ndd &&
-                     (unsigned long long)W2 * 1024ull >= (unsigned long long)a.cut * W;
     // the list the mark pass and the next round read: the scan's list (round
     // 0), the tail CTA's single segment, or the grid's per-CTA segments
     if (!fresh && !ndd) {
@@ -1402,10 +1392,6 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
     if (tail) __syncthreads();
     else if (!grid_barrier(st, kBarrierTimeoutNs, active)) return;
     if (stamp) st->t_round[ph][2 * r - 1] = globaltimer_ns();
-    if (cut) {
-      if (stamp) st->light_cut = 1;
-      break;
-    }
   }
   if (stamp) st->rounds[ph] = r;
 }

@@ -39,8 +39,6 @@ struct DevState {
   int rounds[2];       // Boruvka rounds per phase
   unsigned desc_count; // long-row chunk descriptors emitted by the current scan
   unsigned pad;
-  int light_cut;       // 1 = the light phase stopped early: the heavy scan also keeps
-                       // light entries between light trees
   float quantile;      // learned / quantile modes: filter quantile in [0,1]
   int learned_split;   // learned mode: predicted degree split
   u64 atomics;         // guarded atomicMin issued (stats mode)

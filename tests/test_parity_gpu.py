@@ -20,10 +20,6 @@ MODES = [
     dict(degree_split=1 << 20),
     dict(small_tail=-1),
     dict(small_tail=1 << 30),
-    dict(light_cut=-1),
-    dict(light_cut=1),
-    dict(light_cut=900, mode=E.THRESH_QUANTILE, quantile=0.5),
-    dict(light_cut=1, flags=E.FLAG_DEDUP | E.FLAG_NO_FIND_CACHE, small_tail=-1),
     dict(round_min_tiles=-1),
     dict(round_min_tiles=16, small_tail=-1),
     dict(ctas_per_sm=1),
