@@ -753,8 +753,8 @@ int run_device_once(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d_inMST, const 
   const std::vector<long long> key = {
       g->nodes, g->edges, (long long)(uintptr_t)g->nindex, (long long)(uintptr_t)g->nlist,
       (long long)(uintptr_t)g->eweight, (long long)(uintptr_t)d_inMST, o.threshold_mode, o.threshold,
-      (long long)*(const int*)&qbits, o.degree_split, o.small_tail, o.flags,
-      (long long)ecl_learned_weights_version()};
+      (long long)*(const int*)&qbits, o.degree_split, o.small_tail, o.flags, o.round_min_tiles, o.ctas_per_sm,
+      (long long)(uintptr_t)c->wl[0], (long long)ecl_learned_weights_version()};
   const bool graph_ok = !(o.flags & ECL_FLAG_NO_GRAPH);
   bool replayed = false;
   auto replay = [&]() -> int {
