@@ -11,6 +11,7 @@
 // Parameter blob layout (kMlpParams floats):
 //   W1[16][64], b1[64], W2[64][64], b2[64], W3[64][2], b3[2], mean[16], std[16]
 // Features are standardised with mean/std before the first layer.
+#include <cub/block/block_radix_sort.cuh>
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -32,6 +33,7 @@ static_assert(kParams == ECL_MLP_PARAMS, "parameter blob size");
 constexpr int kTrainable = kOffMean;  // W1..b3
 constexpr int kMB = 64;               // training minibatch
 constexpr int kSample = 4096;         // weight sample for the quantile features
+constexpr float kNoFilterLog2Q = -0.32192809f;  // log2(0.8): predicted quantiles above run unfiltered
 
 int cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return ECL_OK;
@@ -51,14 +53,36 @@ struct FeatAcc {
   unsigned max_deg;
 };
 
-// Degree statistics over all vertices (grid-stride, block reduction, one
-// atomic per block per counter).
-__global__ void k_feat_degrees(const int* nindex, int n, FeatAcc* acc) {
+// The feature pass in one launch: block 0 draws the 4096-entry weight sample
+// and sorts it (a block radix sort, 4 keys per thread) into `sorted`, while
+// the other blocks take the degree statistics over all vertices (grid-stride,
+// block reduction, one atomic per block per counter).
+constexpr int kFeatThreads = 1024;
+constexpr int kFeatKeys = kSample / kFeatThreads;
+
+__global__ void __launch_bounds__(kFeatThreads) k_feat(const int* nindex, int n, const int* eweight, int m,
+                                                        FeatAcc* acc, int* sorted) {
+  typedef cub::BlockRadixSort<int, kFeatThreads, kFeatKeys> SampleSort;
+  __shared__ typename SampleSort::TempStorage sort_tmp;
   __shared__ unsigned long long s[5][32];
   __shared__ unsigned smax[32];
+  if (blockIdx.x == 0) {
+    int keys[kFeatKeys];
+#pragma unroll
+    for (int k = 0; k < kFeatKeys; k++) {
+      const int i = threadIdx.x * kFeatKeys + k;
+      const uint64_t r = ecl_mix64(0xFEA70000ull + (uint64_t)i);
+      keys[k] = m > 0 ? __ldg(eweight + (unsigned)(r % (uint64_t)(unsigned)m)) : 0;
+    }
+    SampleSort(sort_tmp).Sort(keys);  // blocked: thread t holds ranks t * kFeatKeys ...
+#pragma unroll
+    for (int k = 0; k < kFeatKeys; k++) sorted[threadIdx.x * kFeatKeys + k] = keys[k];
+    return;
+  }
   unsigned long long d1 = 0, d2 = 0, z = 0, lo = 0, hi = 0;
   unsigned mx = 0;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+  const int stride = (gridDim.x - 1) * blockDim.x;
+  for (int v = (blockIdx.x - 1) * blockDim.x + threadIdx.x; v < n; v += stride) {
     const int d = __ldg(nindex + v + 1) - __ldg(nindex + v);
     const unsigned ud = d > 0 ? (unsigned)d : 0u;
     d1 += ud;
@@ -100,38 +124,18 @@ __global__ void k_feat_degrees(const int* nindex, int n, FeatAcc* acc) {
   }
 }
 
-// The 16 features, from the degree statistics and a sorted 4096-entry weight
-// sample (one CTA of 1024 threads). The sorted sample is also stored in
-// sorted_out (when not null) so the learned threshold can be read from it.
-__global__ void k_feat_finish(const int* eweight, int n, int m, const FeatAcc* acc, float* out,
-                              int* sorted_out) {
-  __shared__ int samp[kSample];
-  for (int i = threadIdx.x; i < kSample; i += blockDim.x) {
-    const uint64_t r = ecl_mix64(0xFEA70000ull + (uint64_t)i);
-    samp[i] = m > 0 ? eweight[(unsigned)(r % (uint64_t)(unsigned)m)] : 0;
-  }
-  __syncthreads();
-  for (int k = 2; k <= kSample; k <<= 1)
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = threadIdx.x; i < kSample; i += blockDim.x) {
-        const int ixj = i ^ j;
-        if (ixj > i) {
-          const int x = samp[i], y = samp[ixj];
-          if ((x > y) == ((i & k) == 0)) {
-            samp[i] = y;
-            samp[ixj] = x;
-          }
-        }
-      }
-      __syncthreads();
-    }
-  if (sorted_out)
-    for (int i = threadIdx.x; i < kSample; i += blockDim.x) sorted_out[i] = samp[i];
-  if (threadIdx.x != 0) return;
+// Grid of the feature pass: the sorting block plus up to two degree blocks per SM.
+int feat_grid(int nodes, int sms) {
+  return 1 + std::max(1, std::min(sms * 2, (nodes + kFeatThreads - 1) / kFeatThreads));
+}
+
+// The 16 features (one thread), from the degree statistics and the sorted
+// weight sample.
+__device__ void compute_features(int n, int m, const FeatAcc* acc, const int* sorted, float* out) {
   const double dn = (double)n, dm = (double)m;
   const double mean = dm / dn;
   const double var = fmax(0.0, (double)acc->deg_sq / dn - mean * mean);
-  const double wmax = fmax(1.0, (double)samp[kSample - 1]);
+  const double wmax = fmax(1.0, (double)sorted[kSample - 1]);
   const float qs[7] = {0.01f, 0.02f, 0.05f, 0.1f, 0.2f, 0.3f, 0.5f};
   out[0] = (float)log2(dn);
   out[1] = (float)log2(fmax(dm, 1.0));
@@ -142,7 +146,12 @@ __global__ void k_feat_finish(const int* eweight, int n, int m, const FeatAcc* a
   out[6] = (float)((double)acc->low / dn);
   out[7] = (float)((double)acc->high / dn);
   out[8] = (float)(3.0 * dn / fmax(dm, 1.0));  // the reference heuristic's "300% of nodes" quantile
-  for (int i = 0; i < 7; i++) out[9 + i] = (float)((double)samp[(int)(qs[i] * (kSample - 1))] / wmax);
+  for (int i = 0; i < 7; i++) out[9 + i] = (float)((double)sorted[(int)(qs[i] * (kSample - 1))] / wmax);
+}
+
+// The features alone (for training data): one thread.
+__global__ void k_feat_finish(int n, int m, const FeatAcc* acc, const int* sorted, float* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) compute_features(n, m, acc, sorted, out);
 }
 
 // ------------------------------------------------------------------- MLP
@@ -192,11 +201,13 @@ __host__ __device__ __forceinline__ float heuristic_log2_quantile(int n, int m) 
 // One CTA of kH threads: thread j computes hidden unit j of each layer. The
 // decoded quantile selects the light-phase threshold from the sorted weight
 // sample of the feature pass.
-__global__ void k_mlp_apply(const float* p, const float* feat, const int* sorted, int n, int m,
+__global__ void k_mlp_apply(const float* p, const FeatAcc* acc, const int* sorted, int n, int m,
                             ecl::DevState* st) {
-  __shared__ float xs[kIn], h1[kH], h2[kH], y[kOut];
+  __shared__ float fx[kIn], xs[kIn], h1[kH], h2[kH], y[kOut];
   const int j = threadIdx.x;
-  if (j < kIn) xs[j] = (feat[j] - p[kOffMean + j]) / p[kOffStd + j];
+  if (j == 0) compute_features(n, m, acc, sorted, fx);
+  __syncthreads();
+  if (j < kIn) xs[j] = (fx[j] - p[kOffMean + j]) / p[kOffStd + j];
   __syncthreads();
   if (j < kH) {
     float a = p[kOffB1 + j];
@@ -217,9 +228,11 @@ __global__ void k_mlp_apply(const float* p, const float* feat, const int* sorted
   }
   __syncthreads();
   if (j != 0) return;
-  // output 0 (+ the heuristic's log2 quantile) >= -0.02 means "no filter"
+  // output 0 (+ the heuristic's log2 quantile) at or above log2(0.8) means
+  // "no filter": a light phase holding 80 % of the entries or more is not
+  // worth a second phase (measured on the held-out sweeps)
   const float lq = fminf(fmaxf(heuristic_log2_quantile(n, m) + y[0], -10.f), 0.f);
-  const float q = lq >= -0.02f ? 1.0f : exp2f(lq);
+  const float q = lq >= kNoFilterLog2Q ? 1.0f : exp2f(lq);
   st->quantile = q;
   if (q < 1.0f) {
     int idx = (int)(q * (float)(kSample - 1));
@@ -402,10 +415,10 @@ int ecl_learned_prepare(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s, void
     }
   }
   ML_TRY(cudaMemsetAsync(d_acc, 0, sizeof(FeatAcc), s));
-  const int grid = std::max(1, std::min(sms * 4, (g->nodes + 511) / 512));
-  k_feat_degrees<<<grid, 512, 0, s>>>(g->nindex, g->nodes, (FeatAcc*)d_acc);
-  k_feat_finish<<<1, 1024, 0, s>>>(g->eweight, g->nodes, g->edges, (const FeatAcc*)d_acc, d_feat, d_sample);
-  k_mlp_apply<<<1, kH, 0, s>>>(d_params, d_feat, d_sample, g->nodes, g->edges, (ecl::DevState*)st);
+  k_feat<<<feat_grid(g->nodes, sms), kFeatThreads, 0, s>>>(g->nindex, g->nodes, g->eweight, g->edges,
+                                                          (FeatAcc*)d_acc, d_sample);
+  k_mlp_apply<<<1, kH, 0, s>>>(d_params, (const FeatAcc*)d_acc, d_sample, g->nodes, g->edges,
+                               (ecl::DevState*)st);
   ML_TRY(cudaGetLastError());
   return ECL_OK;
 }
@@ -419,18 +432,20 @@ extern "C" int ecl_graph_features(const ecl_graph* g, float* out) {
   ML_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   FeatAcc* acc = nullptr;
   float* f = nullptr;
+  int* sorted = nullptr;
   ML_TRY(cudaMalloc(&acc, sizeof(FeatAcc)));
-  if (cudaMalloc(&f, kIn * sizeof(float)) != cudaSuccess) {
+  if (cudaMalloc(&f, kIn * sizeof(float)) != cudaSuccess || cudaMalloc(&sorted, kSample * sizeof(int)) != cudaSuccess) {
     cudaFree(acc);
+    cudaFree(f);
     return ECL_ERR_ALLOC;
   }
   cudaMemset(acc, 0, sizeof(FeatAcc));
-  const int grid = std::max(1, std::min(sms * 4, (g->nodes + 511) / 512));
-  k_feat_degrees<<<grid, 512>>>(g->nindex, g->nodes, acc);
-  k_feat_finish<<<1, 1024>>>(g->eweight, g->nodes, g->edges, acc, f, nullptr);
+  k_feat<<<feat_grid(g->nodes, sms), kFeatThreads>>>(g->nindex, g->nodes, g->eweight, g->edges, acc, sorted);
+  k_feat_finish<<<1, 32>>>(g->nodes, g->edges, acc, sorted, f);
   cudaError_t e = cudaMemcpy(out, f, kIn * sizeof(float), cudaMemcpyDeviceToHost);
   cudaFree(acc);
   cudaFree(f);
+  cudaFree(sorted);
   return cuda_status(e);
 }
 

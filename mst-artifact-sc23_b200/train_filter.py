@@ -23,7 +23,8 @@
    (filter_training.json) into --out-dir; with --dataset, also the sweep
    tables.
 
-    python train_filter.py --train 2000 --heldout 500 --out-dir <dir>
+    python train_filter.py --train 3000 --heldout 500 --out-dir <dir> --dataset <sweeps.npz>
+    python train_filter.py --eval-only <sweeps.npz> --weights <blob> --out-dir <dir>
 """
 import argparse
 import json
@@ -41,6 +42,11 @@ QUANTILES = [0.005, 0.01, 0.02, 0.03, 0.05, 0.07, 0.1, 0.15, 0.2, 0.3, 0.4, 0.5,
 SPLITS = [4, 8, 16]  # degree splits selecting the scans' E = 4, 8, 16 entries per lane
 FAMILIES = ["grid", "er", "rmat", "rgg"]
 TRAIN_SEED0, HELDOUT_SEED0 = 200_000, 900_000
+
+
+def family_of(seed):
+    """Family name of seed `seed` (make_graph's first draw)."""
+    return FAMILIES[int(np.random.default_rng(seed).integers(4))]
 
 
 def make_graph(seed, nmin, nmax):
@@ -104,10 +110,13 @@ def label(times, n, m, tau=0.03):
                     np.float32)
 
 
+NO_FILTER_LOG2Q = np.log2(0.8)  # as the device decodes: predicted quantiles above 0.8 run unfiltered
+
+
 def predicted_setting(pr, n, m):
     """Grid point nearest the MLP's output (as the device applies it)."""
     lq = min(max(heuristic_log2_quantile(n, m) + float(pr[0]), -10.0), 0.0)
-    q = 1.0 if lq >= -0.02 else 2.0 ** lq
+    q = 1.0 if lq >= NO_FILTER_LOG2Q else 2.0 ** lq
     sp = int(round(min(max(float(pr[1]), 1.0), 6.0)))
     qi = int(np.argmin([abs(np.log2(a) - np.log2(q)) for a in QUANTILES]))
     si = 0 if sp <= 2 else (1 if sp == 3 else 2)  # E = 4 for splits <= 4, 8 for 8, 16 above
@@ -131,27 +140,45 @@ def collect(ctx, count, seed0, nmin, nmax, reps, torch):
                 size=np.array([r["size"] for r in rows]))
 
 
+def load_dataset(path):
+    d = np.load(path, allow_pickle=True)
+    tr = dict(x=d["train_x"], times=d["train_times"], heur=d["train_heur"], size=d["train_size"])
+    ho = dict(x=d["heldout_x"], times=d["heldout_times"], heur=d["heldout_heur"], size=d["heldout_size"])
+    ho["fam"] = list(d["heldout_fam"]) if "heldout_fam" in d.files else [None] * len(ho["x"])
+    return tr, ho
+
+
 def run(args):
     import torch
     # largest graphs drawn: RMAT scale 22 at edge factor 32, ER n_max at degree 32
     ctx = E.Context(1 << 23, 300_000_000)
-    t0 = time.time()
-    tr = collect(ctx, args.train, TRAIN_SEED0, args.nmin, args.nmax, args.reps, torch)
-    print(f"train: {args.train} graphs swept in {time.time() - t0:.0f} s", flush=True)
-    t0 = time.time()
-    ho = collect(ctx, args.heldout, HELDOUT_SEED0, args.nmin, args.nmax, args.reps, torch)
-    print(f"heldout: {args.heldout} graphs swept in {time.time() - t0:.0f} s", flush=True)
-
-    x = tr["x"]
-    mean, std = x.mean(0), x.std(0) + 1e-6
-    y = np.stack([label(t, n, m) for t, (n, m) in zip(tr["times"], tr["size"])])
-    # weight graphs by their solve time (big graphs carry the time) by repeating them
-    rep = np.clip(np.round(tr["heur"] / np.median(tr["heur"])), 1, 8).astype(int)
-    order = np.random.default_rng(args.seed).permutation(int(rep.sum()))
-    xs = np.repeat((x - mean) / std, rep, 0)[order].astype(np.float32)
-    ys = np.repeat(y, rep, 0)[order]
-    p0 = E.mlp_init(args.seed, mean=mean, std=std)
-    p, hist = E.mlp_train(p0, xs, ys, epochs=args.epochs, lr=args.lr)
+    if args.eval_only:
+        # a trained blob and its sweep tables: evaluate the current decoding and
+        # measure the held-out graphs again (the families are drawn again too)
+        tr, ho = load_dataset(args.eval_only)
+        ho["fam"] = [family_of(HELDOUT_SEED0 + i) for i in range(len(ho["x"]))]
+        p = np.fromfile(args.weights, np.float32)
+        hist = None
+        summary_extra = {"evaluated": "the shipped weights on the saved held-out sweeps, and measured again"}
+        args.train, args.heldout = len(tr["x"]), len(ho["x"])
+    else:
+        t0 = time.time()
+        tr = collect(ctx, args.train, TRAIN_SEED0, args.nmin, args.nmax, args.reps, torch)
+        print(f"train: {args.train} graphs swept in {time.time() - t0:.0f} s", flush=True)
+        t0 = time.time()
+        ho = collect(ctx, args.heldout, HELDOUT_SEED0, args.nmin, args.nmax, args.reps, torch)
+        print(f"heldout: {args.heldout} graphs swept in {time.time() - t0:.0f} s", flush=True)
+        x = tr["x"]
+        mean, std = x.mean(0), x.std(0) + 1e-6
+        y = np.stack([label(t, n, m) for t, (n, m) in zip(tr["times"], tr["size"])])
+        # weight graphs by their solve time (big graphs carry the time) by repeating them
+        rep = np.clip(np.round(tr["heur"] / np.median(tr["heur"])), 1, 8).astype(int)
+        order = np.random.default_rng(args.seed).permutation(int(rep.sum()))
+        xs = np.repeat((x - mean) / std, rep, 0)[order].astype(np.float32)
+        ys = np.repeat(y, rep, 0)[order]
+        p0 = E.mlp_init(args.seed, mean=mean, std=std)
+        p, hist = E.mlp_train(p0, xs, ys, epochs=args.epochs, lr=args.lr)
+        summary_extra = {}
 
     # held-out, from the sweep tables: time at the predicted grid point
     pred = E.mlp_forward(p, ho["x"])
@@ -174,11 +201,14 @@ def run(args):
         "train_seeds": [TRAIN_SEED0, TRAIN_SEED0 + args.train - 1],
         "heldout_seeds": [HELDOUT_SEED0, HELDOUT_SEED0 + args.heldout - 1],
         "quantiles": QUANTILES, "splits": SPLITS, "reps": args.reps, "epochs": args.epochs, "lr": args.lr,
-        "loss_first": float(hist[0]), "loss_last": float(hist[-1]),
+        "loss_first": None if hist is None else float(hist[0]),
+        "loss_last": None if hist is None else float(hist[-1]),
         "sweep_heldout": gain(np.ones(len(res), bool)),
         "sweep_heldout_by_family": {f: gain(fams == f) for f in FAMILIES},
         "sweep_heldout_learned_size": gain(gated),
+        "no_filter_above_quantile": 0.8, "learned_min_edges": 1 << 20,
     }
+    summary.update(summary_extra)
 
     # measured: re-solve the held-out graphs with the trained weights loaded
     E.learned_set_weights(p)
@@ -209,10 +239,10 @@ def run(args):
                                              for f in FAMILIES}
     os.makedirs(args.out_dir, exist_ok=True)
     np.asarray(p, np.float32).tofile(os.path.join(args.out_dir, "filter_weights.bin"))
-    if args.dataset:
+    if args.dataset and not args.eval_only:
         np.savez_compressed(args.dataset, train_x=tr["x"], train_times=tr["times"], train_heur=tr["heur"],
                             train_size=tr["size"], heldout_x=ho["x"], heldout_times=ho["times"],
-                            heldout_heur=ho["heur"], heldout_size=ho["size"])
+                            heldout_heur=ho["heur"], heldout_size=ho["size"], heldout_fam=np.array(ho["fam"]))
     with open(os.path.join(args.out_dir, "filter_training.json"), "w") as f:
         json.dump(summary, f, indent=1)
     print(json.dumps(summary), flush=True)
@@ -230,4 +260,7 @@ if __name__ == "__main__":
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out-dir", default=HERE)
     ap.add_argument("--dataset", default=None, help="also write the sweep tables (.npz) here")
+    ap.add_argument("--eval-only", default=None, metavar="DATASET",
+                    help="evaluate --weights on these saved sweep tables and measure the held-out graphs again")
+    ap.add_argument("--weights", default=os.path.join(HERE, "filter_weights.bin"))
     run(ap.parse_args())
