@@ -65,6 +65,9 @@ constexpr int kPairLog = ECL_PAIR_LOG; // parallel-edge table
 constexpr int kPairSlots = 1 << kPairLog;
 constexpr u64 kNoPair = ~0ull;
 constexpr int kSplitAfter = 8;         // find steps before path splitting starts
+#ifndef ECL_FLAT_ROUNDS
+#define ECL_FLAT_ROUNDS 0              // flatten parent[] before rounds with W >= this many x n (0 = never)
+#endif
 #ifndef ECL_L2_HINTS
 #define ECL_L2_HINTS 1                 // evict-first CSR streams, evict-last parent gathers in the scans
 #endif
@@ -1143,7 +1146,8 @@ __device__ __forceinline__ void store_entry(const RoundArgs& a, int4* list, unsi
 __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* in, unsigned W,
                                                int4* out, unsigned* out_ctr, unsigned* kept_ctr,
                                                u64* mcur, u64* mprev, int reset, bool fresh,
-                                               unsigned start, unsigned stride, RoundSmem& s) {
+                                               unsigned start, unsigned stride, RoundSmem& s,
+                                               bool flat = false) {
   constexpr int N = 2 * kEPT;
   const unsigned tile = blockDim.x * kEPT;
   const unsigned ntiles = (W + tile - 1) / tile;
@@ -1185,7 +1189,12 @@ __device__ __forceinline__ void round_find_min(const RoundArgs& a, const int4* i
 #pragma unroll
       for (int k = 0; k < kEPT; k++) keep[k] = in_range[k];
     } else {
-      multi_find<N>(v, vv, a.parent, s, !(a.abl & kAblNoFindCache), keep_ends ? 0 : kSplitAfter);
+      if (flat) {  // parent[] was just flattened: one load names the root
+#pragma unroll
+        for (int i = 0; i < N; i++) v[i] = vv[i] ? __ldcg(a.parent + v[i]) : v[i];
+      } else {
+        multi_find<N>(v, vv, a.parent, s, !(a.abl & kAblNoFindCache), keep_ends ? 0 : kSplitAfter);
+      }
 #pragma unroll
       for (int k = 0; k < kEPT; k++) {
         keep[k] = in_range[k] && v[2 * k] != v[2 * k + 1];
@@ -1363,8 +1372,20 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
     // reps: those rounds clear the whole previous array
     const bool dense = (a.abl & kAblKeepEnds) || (!tail && 4ull * W >= (unsigned long long)a.nodes);
     const int reset = r == 0 ? kResetNone : (dense ? kResetDense : kResetSparse);
+    // A round whose entries outnumber the vertices ECL_FLAT_ROUNDS times first
+    // points every vertex at its root (one grid-stride pass; roots do not
+    // change between passes), so each of its finds is a single load.
+    const bool flat = ECL_FLAT_ROUNDS > 0 && !fresh && !tail && !(a.abl & kAblKeepEnds) &&
+                      (unsigned long long)W >= (unsigned long long)ECL_FLAT_ROUNDS * (unsigned)a.nodes;
+    if (flat) {
+      for (int v = (int)(start * blockDim.x + threadIdx.x); v < a.nodes; v += (int)(stride * blockDim.x)) {
+        const int rt = find_ro(v, a.parent);
+        if (rt != v) __stcg(a.parent + v, rt);
+      }
+      if (!grid_barrier(st, kBarrierTimeoutNs, active)) return;
+    }
     round_find_min(a, in, W, out, &st->wl_count[ph][r + 1], &st->wl_kept[ph][r + 1], mcur, mprev, reset,
-                   fresh, start, stride, s);
+                   fresh, start, stride, s, flat);
     if (fresh && blockIdx.x == 0 && threadIdx.x == 0) {  // the scan's list is round 0's output
       st->wl_count[ph][1] = W;
       st->wl_kept[ph][1] = st->scan_kept[ph];
