@@ -201,10 +201,15 @@ __host__ __device__ __forceinline__ float heuristic_log2_quantile(int n, int m) 
 // One CTA of kH threads: thread j computes hidden unit j of each layer. The
 // decoded quantile selects the light-phase threshold from the sorted weight
 // sample of the feature pass.
-__global__ void k_mlp_apply(const float* p, const FeatAcc* acc, const int* sorted, int n, int m,
+__global__ void k_mlp_apply(const float* pg, const FeatAcc* acc, const int* sorted, int n, int m,
                             ecl::DevState* st) {
+  // the whole parameter blob (21 KB) is staged in shared memory first, so the
+  // layers read it at shared-memory latency instead of one global load per
+  // multiply-add
+  __shared__ float p[kParams];
   __shared__ float fx[kIn], xs[kIn], h1[kH], h2[kH], y[kOut];
   const int j = threadIdx.x;
+  for (int i = j; i < kParams; i += blockDim.x) p[i] = __ldg(pg + i);
   if (j == 0) compute_features(n, m, acc, sorted, fx);
   __syncthreads();
   if (j < kIn) xs[j] = (fx[j] - p[kOffMean + j]) / p[kOffStd + j];
@@ -417,7 +422,7 @@ int ecl_learned_prepare(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s, void
   ML_TRY(cudaMemsetAsync(d_acc, 0, sizeof(FeatAcc), s));
   k_feat<<<feat_grid(g->nodes, sms), kFeatThreads, 0, s>>>(g->nindex, g->nodes, g->eweight, g->edges,
                                                           (FeatAcc*)d_acc, d_sample);
-  k_mlp_apply<<<1, kH, 0, s>>>(d_params, (const FeatAcc*)d_acc, d_sample, g->nodes, g->edges,
+  k_mlp_apply<<<1, 256, 0, s>>>(d_params, (const FeatAcc*)d_acc, d_sample, g->nodes, g->edges,
                                (ecl::DevState*)st);
   ML_TRY(cudaGetLastError());
   return ECL_OK;
