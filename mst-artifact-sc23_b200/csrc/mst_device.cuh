@@ -65,8 +65,12 @@ constexpr int kPairLog = ECL_PAIR_LOG; // parallel-edge table
 constexpr int kPairSlots = 1 << kPairLog;
 constexpr u64 kNoPair = ~0ull;
 constexpr int kSplitAfter = 8;         // find steps before path splitting starts
+// Rounds whose worklist holds at least ECL_FLAT_ROUNDS x n entries first
+// point every vertex at its root, so their finds are single loads (RMAT-22:
+// 11 % faster with the reference heuristic's schedule, 1 % with the learned
+// one; flattening from W >= n already was slower than from W >= 2n)
 #ifndef ECL_FLAT_ROUNDS
-#define ECL_FLAT_ROUNDS 0              // flatten parent[] before rounds with W >= this many x n (0 = never)
+#define ECL_FLAT_ROUNDS 2
 #endif
 #ifndef ECL_L2_HINTS
 #define ECL_L2_HINTS 1                 // evict-first CSR streams, evict-last parent gathers in the scans
