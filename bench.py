@@ -477,6 +477,11 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    # Every device operation of the bench (solves, L2 flushes, copies) goes to
+    # one stream. torch's default stream has the handle 0, which the library
+    # reads as "the context's own stream", and that stream does not order
+    # against torch's: a flush there could overlap the timed solve.
+    torch.cuda.set_stream(torch.cuda.Stream(device=dev))
 
     kind, kw, desc = WORKLOADS[args.workload]
     t0 = time.perf_counter()

@@ -155,6 +155,9 @@ def test_device_entry_point_with_torch_buffers(ctx):
     s = torch.cuda.current_stream().cuda_stream
     for _ in range(2):
         out.fill_(7)
+        # torch's default stream is handle 0, which the library reads as the
+        # context's own stream: wait for torch's work before the solve
+        torch.cuda.synchronize()
         ctx.run_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(),
                        stream=s)
         torch.cuda.synchronize()
@@ -348,6 +351,7 @@ def test_repeated_solve_is_captured_and_replayed(ctx):
             w = g.eweight if step < 3 else (g.eweight ^ 0x5A5A).astype(np.int32)
             ew.copy_(torch.from_numpy(w))
             out.fill_(7)
+            torch.cuda.synchronize()  # torch's stream (handle 0) is not the one the solve runs on
             st = ctx.run_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(),
                                 opts=o, stream=s, stats=True)
             want, _, _ = O.oracle_mst(g.nindex, g.nlist, w, st["threshold"], st["filtered"])
@@ -384,6 +388,7 @@ def test_one_direction_input_grows_the_worklists(k):
     for stats in (True, False):
         with E.Context(g.nodes, g.edges) as c:
             out = torch.full((g.edges,), 7, dtype=torch.uint8, device=dev)
+            torch.cuda.synchronize()
             c.run_device(g.nodes, g.edges, ni.data_ptr(), nl.data_ptr(), ew.data_ptr(), out.data_ptr(),
                          stream=torch.cuda.current_stream().cuda_stream, stats=stats)
             c.sync()

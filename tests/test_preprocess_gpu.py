@@ -142,6 +142,7 @@ def test_device_generated_graph_solves_to_the_oracle_forest():
     with E.gen_rmat_device(15, 16, 0.57, 0.19, 0.19, 2, 1 << 24) as d:
         h = d.to_host()
         out = torch.zeros(d.edges, dtype=torch.uint8, device="cuda:0")
+        torch.cuda.synchronize()
         with E.Context(d.nodes, d.edges) as ctx:
             ctx.run_device(d.nodes, d.edges, d.d_nindex, d.d_nlist, d.d_eweight, out.data_ptr(),
                            stream=torch.cuda.current_stream().cuda_stream)
