@@ -25,6 +25,9 @@
 
     python train_filter.py --train 3000 --heldout 500 --out-dir <dir> --dataset <sweeps.npz>
     python train_filter.py --eval-only <sweeps.npz> --weights <blob> --out-dir <dir>
+    python train_filter.py --nmin 4000000 --nmax 33554432 --seed-offset 50000 \
+        --train 500 --heldout 150 --out-dir <dir> --dataset <large.npz>
+    python train_filter.py --from-datasets <sweeps.npz> <large.npz> --out-dir <dir>
 """
 import argparse
 import json
@@ -61,8 +64,10 @@ def make_graph(seed, nmin, nmax):
     if fam == 1:
         return E.gen_er_device(n, float(rng.choice([8, 16, 32])), seed, wmax), "er"
     if fam == 2:
-        return E.gen_rmat_device(max(10, int(round(np.log2(n)))), int(rng.choice([8, 16, 32])), 0.57, 0.19, 0.19,
-                                 seed, wmax), "rmat"
+        scale = max(10, int(round(np.log2(n))))
+        ef = int(rng.choice([8, 16, 32]))
+        ef = min(ef, (1 << 30) >> (scale + 1))  # at most 2^30 entries (edge factor 16 at scale 25)
+        return E.gen_rmat_device(scale, ef, 0.57, 0.19, 0.19, seed, wmax), "rmat"
     return E.gen_rgg2d_device(n, 3.0, seed, wmax), "rgg"
 
 
@@ -141,44 +146,98 @@ def collect(ctx, count, seed0, nmin, nmax, reps, torch):
 
 
 def load_dataset(path):
+    """Sweep tables of a dataset. Held-out graph i was drawn from seed
+    heldout_seed0 + i with vertex counts in [nmin, nmax] (datasets without
+    that record are the first sweep: seeds 900000.., 10^4..4*10^6)."""
     d = np.load(path, allow_pickle=True)
     tr = dict(x=d["train_x"], times=d["train_times"], heur=d["train_heur"], size=d["train_size"])
     ho = dict(x=d["heldout_x"], times=d["heldout_times"], heur=d["heldout_heur"], size=d["heldout_size"])
-    ho["fam"] = list(d["heldout_fam"]) if "heldout_fam" in d.files else [None] * len(ho["x"])
+    meta = d["meta"].tolist() if "meta" in d.files else dict(heldout_seed0=HELDOUT_SEED0, nmin=10_000, nmax=4_000_000)
+    k = len(ho["x"])
+    ho["seed"] = [meta["heldout_seed0"] + i for i in range(k)]
+    ho["nmin"] = [meta["nmin"]] * k
+    ho["nmax"] = [meta["nmax"]] * k
+    ho["fam"] = [family_of(sd) for sd in ho["seed"]]
     return tr, ho
+
+
+def seed_ranges(ho):
+    """[first seed, last seed, nmin, nmax] of each held-out sweep in `ho`."""
+    r = {}
+    for sd, lo, hi in zip(ho["seed"], ho["nmin"], ho["nmax"]):
+        a, b = r.get((lo, hi), (sd, sd))
+        r[(lo, hi)] = (min(a, sd), max(b, sd))
+    return [[int(a), int(b), int(lo), int(hi)] for (lo, hi), (a, b) in sorted(r.items())]
+
+
+def concat(parts):
+    out = {}
+    for key in parts[0]:
+        vals = [p[key] for p in parts]
+        out[key] = np.concatenate(vals) if isinstance(vals[0], np.ndarray) else sum((list(v) for v in vals), [])
+    return out
+
+
+def time_weight(tr):
+    """Repeat count of each graph: its solve time over the sweep's median,
+    1..8 (big graphs carry the time)."""
+    return np.clip(np.round(tr["heur"] / np.median(tr["heur"])), 1, 8).astype(int)
+
+
+def train_on(tr, seed, epochs, lr):
+    """The MLP trained by the library's CUDA kernel on sweep tables."""
+    x = tr["x"]
+    mean, std = x.mean(0), x.std(0) + 1e-6
+    y = np.stack([label(t, n, m) for t, (n, m) in zip(tr["times"], tr["size"])])
+    rep = tr["rep"] if "rep" in tr else time_weight(tr)
+    order = np.random.default_rng(seed).permutation(int(rep.sum()))
+    xs = np.repeat((x - mean) / std, rep, 0)[order].astype(np.float32)
+    ys = np.repeat(y, rep, 0)[order]
+    p0 = E.mlp_init(seed, mean=mean, std=std)
+    return E.mlp_train(p0, xs, ys, epochs=epochs, lr=lr)
 
 
 def run(args):
     import torch
-    # largest graphs drawn: RMAT scale 22 at edge factor 32, ER n_max at degree 32
-    ctx = E.Context(1 << 23, 300_000_000)
-    if args.eval_only:
-        # a trained blob and its sweep tables: evaluate the current decoding and
-        # measure the held-out graphs again (the families are drawn again too)
-        tr, ho = load_dataset(args.eval_only)
-        ho["fam"] = [family_of(HELDOUT_SEED0 + i) for i in range(len(ho["x"]))]
-        p = np.fromfile(args.weights, np.float32)
-        hist = None
-        summary_extra = {"evaluated": "the shipped weights on the saved held-out sweeps, and measured again"}
+    summary_extra = {}
+    parts = None
+    if args.eval_only or args.from_datasets:
+        parts = [load_dataset(d) for d in (args.from_datasets or [args.eval_only])]
+        args.nmin = min(min(h["nmin"]) for _, h in parts)
+        args.nmax = max(max(h["nmax"]) for _, h in parts)
+    # largest graphs drawn: RMAT scale 22 at edge factor 32 and ER n_max at degree
+    # 32; with vertex counts up to 2^25, RMAT scale 25 at edge factor 16 and ER
+    # 2^25 at degree 32 (about 1.07e9 entries)
+    big = args.nmax > 4_200_000
+    if big and args.nmax > 1 << 25:
+        raise SystemExit("--nmax above 2^25 needs a larger context")
+    ctx = E.Context(1 << 25, 1_100_000_000) if big else E.Context(1 << 23, 300_000_000)
+    if parts:
+        # saved sweep tables: train on their union (or take the shipped weights),
+        # evaluate the current decoding, and measure the held-out graphs again
+        for t, _ in parts:
+            t["rep"] = time_weight(t)  # each sweep weighted against its own median
+        tr = concat([t for t, _ in parts])
+        ho = concat([h for _, h in parts])
+        if args.eval_only:
+            p = np.fromfile(args.weights, np.float32)
+            hist = None
+            summary_extra["evaluated"] = "the shipped weights on the saved held-out sweeps, and measured again"
+        else:
+            p, hist = train_on(tr, args.seed, args.epochs, args.lr)
+            summary_extra["datasets"] = [os.path.basename(d) for d in args.from_datasets]
         args.train, args.heldout = len(tr["x"]), len(ho["x"])
     else:
         t0 = time.time()
-        tr = collect(ctx, args.train, TRAIN_SEED0, args.nmin, args.nmax, args.reps, torch)
+        tr = collect(ctx, args.train, TRAIN_SEED0 + args.seed_offset, args.nmin, args.nmax, args.reps, torch)
         print(f"train: {args.train} graphs swept in {time.time() - t0:.0f} s", flush=True)
         t0 = time.time()
-        ho = collect(ctx, args.heldout, HELDOUT_SEED0, args.nmin, args.nmax, args.reps, torch)
+        h0 = HELDOUT_SEED0 + args.seed_offset
+        ho = collect(ctx, args.heldout, h0, args.nmin, args.nmax, args.reps, torch)
+        ho["seed"] = [h0 + i for i in range(args.heldout)]
+        ho["nmin"], ho["nmax"] = [args.nmin] * args.heldout, [args.nmax] * args.heldout
         print(f"heldout: {args.heldout} graphs swept in {time.time() - t0:.0f} s", flush=True)
-        x = tr["x"]
-        mean, std = x.mean(0), x.std(0) + 1e-6
-        y = np.stack([label(t, n, m) for t, (n, m) in zip(tr["times"], tr["size"])])
-        # weight graphs by their solve time (big graphs carry the time) by repeating them
-        rep = np.clip(np.round(tr["heur"] / np.median(tr["heur"])), 1, 8).astype(int)
-        order = np.random.default_rng(args.seed).permutation(int(rep.sum()))
-        xs = np.repeat((x - mean) / std, rep, 0)[order].astype(np.float32)
-        ys = np.repeat(y, rep, 0)[order]
-        p0 = E.mlp_init(args.seed, mean=mean, std=std)
-        p, hist = E.mlp_train(p0, xs, ys, epochs=args.epochs, lr=args.lr)
-        summary_extra = {}
+        p, hist = train_on(tr, args.seed, args.epochs, args.lr)
 
     # held-out, from the sweep tables: time at the predicted grid point
     pred = E.mlp_forward(p, ho["x"])
@@ -198,8 +257,7 @@ def run(args):
 
     summary = {
         "train_graphs": args.train, "heldout_graphs": args.heldout, "nmin": args.nmin, "nmax": args.nmax,
-        "train_seeds": [TRAIN_SEED0, TRAIN_SEED0 + args.train - 1],
-        "heldout_seeds": [HELDOUT_SEED0, HELDOUT_SEED0 + args.heldout - 1],
+        "heldout_seed_ranges": seed_ranges(ho),
         "quantiles": QUANTILES, "splits": SPLITS, "reps": args.reps, "epochs": args.epochs, "lr": args.lr,
         "loss_first": None if hist is None else float(hist[0]),
         "loss_last": None if hist is None else float(hist[-1]),
@@ -214,7 +272,7 @@ def run(args):
     E.learned_set_weights(p)
     meas = []
     for i in range(args.heldout):
-        dg, fam = make_graph(HELDOUT_SEED0 + i, args.nmin, args.nmax)
+        dg, fam = make_graph(ho["seed"][i], ho["nmin"][i], ho["nmax"][i])
         out = torch.empty(max(dg.edges, 1), dtype=torch.uint8, device="cuda:0")
         th = tl = 1e30
         for _ in range(2):  # interleaved, best of each
@@ -237,12 +295,19 @@ def run(args):
     summary["measured_heldout_learned_size"] = mgain(big)
     summary["measured_heldout_by_family"] = {f: mgain([fm == f and b for (fm, _, _, _), b in zip(meas, big)])
                                              for f in FAMILIES}
+    large = [n > 4_200_000 for n in ho["size"][:, 0]]
+    if any(large):
+        summary["measured_heldout_above_4M_vertices"] = mgain(large)
+        summary["measured_heldout_above_4M_by_family"] = {
+            f: mgain([fm == f and b for (fm, _, _, _), b in zip(meas, large)]) for f in FAMILIES}
     os.makedirs(args.out_dir, exist_ok=True)
     np.asarray(p, np.float32).tofile(os.path.join(args.out_dir, "filter_weights.bin"))
-    if args.dataset and not args.eval_only:
+    if args.dataset and not (args.eval_only or args.from_datasets):
+        meta = dict(train_seed0=TRAIN_SEED0 + args.seed_offset, heldout_seed0=HELDOUT_SEED0 + args.seed_offset,
+                    nmin=args.nmin, nmax=args.nmax)
         np.savez_compressed(args.dataset, train_x=tr["x"], train_times=tr["times"], train_heur=tr["heur"],
                             train_size=tr["size"], heldout_x=ho["x"], heldout_times=ho["times"],
-                            heldout_heur=ho["heur"], heldout_size=ho["size"], heldout_fam=np.array(ho["fam"]))
+                            heldout_heur=ho["heur"], heldout_size=ho["size"], meta=np.array(meta, dtype=object))
     with open(os.path.join(args.out_dir, "filter_training.json"), "w") as f:
         json.dump(summary, f, indent=1)
     print(json.dumps(summary), flush=True)
@@ -263,4 +328,8 @@ if __name__ == "__main__":
     ap.add_argument("--eval-only", default=None, metavar="DATASET",
                     help="evaluate --weights on these saved sweep tables and measure the held-out graphs again")
     ap.add_argument("--weights", default=os.path.join(HERE, "filter_weights.bin"))
+    ap.add_argument("--from-datasets", nargs="+", default=None, metavar="DATASET",
+                    help="train on the union of these saved sweep tables instead of sweeping")
+    ap.add_argument("--seed-offset", type=int, default=0,
+                    help="added to the training and held-out seed ranges (a second, disjoint sweep)")
     run(ap.parse_args())
