@@ -358,10 +358,10 @@ int ecl_mst_run_device(ecl_mst_ctx* ctx, const ecl_graph* d_graph,
  *   - ECL_THRESH_LEARNED takes the reference heuristic here, as
  *     ecl_mst_run_device does for graphs below its learned-schedule cut-off
  *     (the feature pass needs scratch this entry point does not hold);
- *   - the first call on a device resolves the scratch address on that device
- *     (make it before any stream capture) and keeps it for the life of the
- *     process: do not call it again on a device after cudaDeviceReset, which
- *     unloads the module that owns the array; the call enqueues on `stream`
+ *   - every call looks up the scratch array's address on the current device
+ *     (a device reset reloads the module that owns it); the first call on a
+ *     device also reads its attributes, so make it before any stream
+ *     capture; the call enqueues on `stream`
  *     (cudaStream_t, NULL = legacy default stream) and returns after the solve
  *     finished, with device-side errors as its status;
  *   - all calls share the one scratch array: calls that overlap on the GPU

@@ -1061,9 +1061,12 @@ int na_setup(int dev, NaDevice** out) {
   if (dev < 0 || dev >= kNaMaxDevices) return ECL_ERR_UNSUPPORTED;
   std::lock_guard<std::mutex> lock(g_na_mu);
   NaDevice& d = g_na_dev[dev];
+  // The scratch array's address is looked up on every call: a device reset
+  // reloads the module, and the array then lives elsewhere.
+  void* p = nullptr;
+  ECL_CUDA_TRY(cudaGetSymbolAddress(&p, g_na_scratch));
+  d.base = (unsigned char*)p;
   if (!d.ready) {
-    void* p = nullptr;
-    ECL_CUDA_TRY(cudaGetSymbolAddress(&p, g_na_scratch));
     int coop = 0;
     ECL_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     if (!coop) return ECL_ERR_UNSUPPORTED;
@@ -1072,7 +1075,6 @@ int na_setup(int dev, NaDevice** out) {
     int ps = prepare_scan_kernels();
     if (ps) return ps;
     if (d.round_grid <= 0) return ECL_ERR_CUDA;
-    d.base = (unsigned char*)p;
     d.ready = true;
   }
   *out = &d;
