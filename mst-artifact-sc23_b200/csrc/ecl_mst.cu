@@ -14,7 +14,17 @@
 #include "internal.h"
 #include "mst_device.cuh"
 #include "batch_device.cuh"
+#include <functional>
 #include <vector>
+
+// Learned threshold/split (learned.cu). ecl_learned_sample uploads changed
+// weights and sorts the weight sample; ecl_learned_apply computes the
+// features from it and from k_prep's degree statistics and runs the trained
+// MLP, writing DevState::threshold, filtered, quantile and split.
+int ecl_learned_sample(ecl_mst_ctx* c, const ecl_graph* d_graph, cudaStream_t s);
+int ecl_learned_apply(ecl_mst_ctx* c, const ecl_graph* d_graph, cudaStream_t s, void* st);
+int ecl_learned_upload(ecl_mst_ctx* c, cudaStream_t s);
+unsigned ecl_learned_weights_version();
 
 using namespace ecl;
 
@@ -34,7 +44,7 @@ struct ecl_mst_ctx {
   cudaStream_t stream = nullptr;
   // the learned schedule's feature pass runs on `side`, beside k_prep
   cudaStream_t side = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr, prep_done = nullptr;
   // the last solve's key, and the captured solve (CUDA graph) with its key
   std::vector<long long> last_key, exec_key;
   cudaGraphExec_t exec = nullptr;
@@ -194,7 +204,11 @@ int64_t first_v_entries(int64_t edges) {
 
 // k_prep, then the fill scan that completes the tile->vertex table
 // (first_v: pa.tiles + 1 entries, then room for the chunk maxima).
-int enqueue_prep(const PrepArgs& pa, int sm_count, cudaStream_t s, const cudaAccessPolicyWindow* win = nullptr) {
+// k_prep, then the max scan of the tile->vertex table. `after_prep`, when
+// given, is enqueued between the two (the learned schedule forks its MLP off
+// there, once k_prep's degree statistics are complete).
+int enqueue_prep(const PrepArgs& pa, int sm_count, cudaStream_t s, const cudaAccessPolicyWindow* win = nullptr,
+                 const std::function<int()>& after_prep = nullptr) {
   ECL_CUDA_TRY(cudaMemsetAsync(pa.first_v, 0, sizeof(int) * (size_t)pa.tiles, s));
   const int prep_grid = (int)std::min<int64_t>((pa.nodes + kThreads - 1) / kThreads, (int64_t)sm_count * 16);
   if (win) {
@@ -202,6 +216,11 @@ int enqueue_prep(const PrepArgs& pa, int sm_count, cudaStream_t s, const cudaAcc
     if (st) return st;
   } else {
     k_prep<<<std::max(prep_grid, 1), kThreads, 0, s>>>(pa);
+  }
+  ECL_CUDA_TRY(cudaGetLastError());
+  if (after_prep) {
+    const int st = after_prep();
+    if (st) return st;
   }
   const int chunks = (pa.tiles + kFillChunk - 1) / kFillChunk;
   int* chunk_max = pa.first_v + pa.tiles + 1;
@@ -280,6 +299,7 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   if ((st = cuda_status(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)))) return fail(st);
   if ((st = cuda_status(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming)))) return fail(st);
   if ((st = cuda_status(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming)))) return fail(st);
+  if ((st = cuda_status(cudaEventCreateWithFlags(&c->prep_done, cudaEventDisableTiming)))) return fail(st);
   const size_t slot_bytes = (size_t)max_nodes * (2 * sizeof(u64) + sizeof(int));
   if ((st = cuda_status(cudaMalloc(&c->slots, slot_bytes)))) return fail(st);
   c->l2_persist_max = prop.persistingL2CacheMaxSize > 0 ? (size_t)prop.persistingL2CacheMaxSize : 0;
@@ -290,7 +310,7 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   if ((st = cuda_status(cudaMalloc(&c->st, sizeof(DevState))))) return fail(st);
   if ((st = cuda_status(cudaMalloc(&c->ml_params, ECL_MLP_PARAMS * sizeof(float))))) return fail(st);
   if ((st = cuda_status(cudaMalloc(&c->ml_feat, ECL_MLP_INPUTS * sizeof(float))))) return fail(st);
-  if ((st = cuda_status(cudaMalloc(&c->ml_acc, 64)))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->ml_acc, sizeof(FeatAcc))))) return fail(st);
   if ((st = cuda_status(cudaMalloc(&c->ml_sample, 4096 * sizeof(int))))) return fail(st);
   if ((st = cuda_status(cudaHostAlloc(&c->st_host, sizeof(DevState), cudaHostAllocDefault))))
     return fail(st);
@@ -346,6 +366,7 @@ extern "C" void ecl_mst_ctx_destroy(ecl_mst_ctx* c) {
   if (c->exec) cudaGraphExecDestroy(c->exec);
   if (c->fork) cudaEventDestroy(c->fork);
   if (c->join) cudaEventDestroy(c->join);
+  if (c->prep_done) cudaEventDestroy(c->prep_done);
   if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -468,10 +489,29 @@ bool l2_window(const ecl_mst_ctx* c, const Slots& sl, bool parent_only, cudaAcce
   return true;
 }
 
-// `join`, when set, is recorded on the stream that runs the learned
-// schedule's feature pass; the light scan waits for it, k_prep does not.
+// The learned schedule's steps around k_prep. The weight sample is sorted on
+// `side` from the start of the solve (ecl_learned_sample); k_prep gathers the
+// degree statistics into `acc` on the solve's stream; the MLP then runs on
+// `side` beside the fill scan, and the light scan waits for it.
+struct LearnedPlan {
+  cudaStream_t side;
+  cudaEvent_t prep_done, join;
+  FeatAcc* acc;
+};
+
+// Start of a learned solve on stream q: zero the degree accumulator (before
+// k_prep adds to it), then fork the side stream and sort the weight sample
+// there. Fills lp->acc.
+int learned_fork(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t q, LearnedPlan* lp) {
+  lp->acc = static_cast<FeatAcc*>(c->ml_acc);
+  ECL_CUDA_TRY(cudaMemsetAsync(lp->acc, 0, sizeof(FeatAcc), q));
+  ECL_CUDA_TRY(cudaEventRecord(c->fork, q));
+  ECL_CUDA_TRY(cudaStreamWaitEvent(lp->side, c->fork, 0));
+  return ecl_learned_sample(c, g, lp->side);
+}
+
 int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, const mst_opts* o,
-                  cudaStream_t s, bool timed, cudaEvent_t join = nullptr) {
+                  cudaStream_t s, bool timed, const LearnedPlan* lp = nullptr) {
   const int n = g->nodes, m = g->edges;
   const int split = o->degree_split > 0 ? o->degree_split : kDefaultSplit;
   const bool device_split = o->threshold_mode == ECL_THRESH_LEARNED;
@@ -483,7 +523,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   const bool l2 = (o->flags & ECL_FLAG_L2_PERSIST) != 0;
   const cudaAccessPolicyWindow* win_all = l2 && l2_window(c, sl, false, &w_all) ? &w_all : nullptr;
   const cudaAccessPolicyWindow* win_par = l2 && l2_window(c, sl, true, &w_par) ? &w_par : nullptr;
-  PrepArgs pa;
+  PrepArgs pa{};
   pa.nodes = n;
   pa.edges = m;
   pa.nindex = g->nindex;
@@ -498,9 +538,20 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   pa.split = split;
   pa.quantile = o->quantile;
   pa.st = c->st;
+  pa.feat = lp ? lp->acc : nullptr;
   int st;
-  if ((st = enqueue_prep(pa, c->sm_count, s, win_all))) return st;
-  if (join) ECL_CUDA_TRY(cudaStreamWaitEvent(s, join, 0));
+  std::function<int()> fork_mlp;
+  if (lp)
+    fork_mlp = [&]() -> int {
+      ECL_CUDA_TRY(cudaEventRecord(lp->prep_done, s));
+      ECL_CUDA_TRY(cudaStreamWaitEvent(lp->side, lp->prep_done, 0));
+      const int r = ecl_learned_apply(c, g, lp->side, c->st);
+      if (r) return r;
+      ECL_CUDA_TRY(cudaEventRecord(lp->join, lp->side));
+      return ECL_OK;
+    };
+  if ((st = enqueue_prep(pa, c->sm_count, s, win_all, fork_mlp))) return st;
+  if (lp) ECL_CUDA_TRY(cudaStreamWaitEvent(s, lp->join, 0));
   const bool no_tuples = (o->flags & (ECL_FLAG_NO_TUPLES | ECL_FLAG_NO_EDGE_BASED)) == ECL_FLAG_NO_TUPLES;
   if (no_tuples) {  // the vertex of every entry, for the gathers of the rounds
     const int sgrid = (int)std::min<int64_t>(((int64_t)m + kThreads - 1) / kThreads, (int64_t)c->sm_count * 16);
@@ -670,12 +721,6 @@ int check_opts(const mst_opts* o) {
 
 }  // namespace
 
-// Learned threshold/split: extracts graph features on the device and runs the
-// trained MLP, writing DevState::quantile and DevState::learned_split.
-int ecl_learned_prepare(ecl_mst_ctx* c, const ecl_graph* d_graph, cudaStream_t s, void* st);
-int ecl_learned_upload(ecl_mst_ctx* c, cudaStream_t s);
-unsigned ecl_learned_weights_version();
-
 int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, float** feat, void** acc, int** sample,
                             unsigned** version, int* sm_count) {
   *sample = c->ml_sample;
@@ -730,17 +775,10 @@ int run_device_once(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d_inMST, const 
     ECL_CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevState), q));
     // the timed window starts before the learned schedule's feature pass
     if (inner_events) ECL_CUDA_TRY(cudaEventRecord(c->ev[0], q));
-    cudaEvent_t join = nullptr;
-    if (o.threshold_mode == ECL_THRESH_LEARNED) {
-      // the feature pass and the MLP run on the side stream, beside k_prep
-      ECL_CUDA_TRY(cudaEventRecord(c->fork, q));
-      ECL_CUDA_TRY(cudaStreamWaitEvent(c->side, c->fork, 0));
-      int r = ecl_learned_prepare(c, g, c->side, c->st);
-      if (r) return r;
-      ECL_CUDA_TRY(cudaEventRecord(c->join, c->side));
-      join = c->join;
-    }
-    return enqueue_solve(c, g, d_inMST, &o, q, inner_events, join);
+    if (o.threshold_mode != ECL_THRESH_LEARNED) return enqueue_solve(c, g, d_inMST, &o, q, inner_events);
+    LearnedPlan lp{c->side, c->prep_done, c->join, nullptr};
+    const int r = learned_fork(c, g, q, &lp);
+    return r ? r : enqueue_solve(c, g, d_inMST, &o, q, inner_events, &lp);
   };
   // A solve repeated with the same graph, buffers and options (benchmarks,
   // iterative callers) is captured once as a CUDA graph and then replayed
@@ -1118,7 +1156,7 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   ECL_CUDA_TRY(cudaMemsetAsync(dst, 0, sizeof(DevState), s));
   const int split = o.degree_split > 0 ? o.degree_split : kDefaultSplit;
   const int tiles = (int)(((int64_t)m + kGran - 1) / kGran);
-  PrepArgs pa;
+  PrepArgs pa{};
   pa.nodes = n;
   pa.edges = m;
   pa.nindex = g->nindex;
@@ -1402,18 +1440,16 @@ int batch_enqueue(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST, const 
                         b->eweight + b->edge_off[g]};
         ECL_CUDA_TRY(cudaMemsetAsync(c->big->st, 0, sizeof(DevState), q));
         mst_opts go = lo;
-        cudaEvent_t join = nullptr;
+        LearnedPlan lp{c->big->side, c->big->prep_done, c->big->join, nullptr};
+        const LearnedPlan* plan = nullptr;
         if (learned && dg.edges >= kLearnedMinEdges) {
-          ECL_CUDA_TRY(cudaEventRecord(c->big->fork, q));
-          ECL_CUDA_TRY(cudaStreamWaitEvent(c->big->side, c->big->fork, 0));
-          int r = ecl_learned_prepare(c->big, &dg, c->big->side, c->big->st);
+          const int r = learned_fork(c->big, &dg, q, &lp);
           if (r) return r;
-          ECL_CUDA_TRY(cudaEventRecord(c->big->join, c->big->side));
-          join = c->big->join;
+          plan = &lp;
         } else if (go.threshold_mode == ECL_THRESH_LEARNED) {
           go.threshold_mode = ECL_THRESH_HEURISTIC;
         }
-        int r = enqueue_solve(c->big, &dg, d_inMST + b->edge_off[g], &go, q, false, join);
+        int r = enqueue_solve(c->big, &dg, d_inMST + b->edge_off[g], &go, q, false, plan);
         if (r) return r;
         k_or_error<<<1, 1, 0, q>>>(c->big->st, c->st);
         ECL_CUDA_TRY(cudaGetLastError());

@@ -48,80 +48,51 @@ int cuda_status(cudaError_t e) {
   } while (0)
 
 // ------------------------------------------------------------- features
-struct FeatAcc {
-  unsigned long long deg_sum, deg_sq, zero, low, high;
-  unsigned max_deg;
-};
+using ecl::FeatAcc;
+using ecl::FeatPart;
 
-// The feature pass in one launch: block 0 draws the 4096-entry weight sample
-// and sorts it (a block radix sort, 4 keys per thread) into `sorted`, while
-// the other blocks take the degree statistics over all vertices (grid-stride,
-// block reduction, one atomic per block per counter).
 constexpr int kFeatThreads = 1024;
 constexpr int kFeatKeys = kSample / kFeatThreads;
 
-__global__ void __launch_bounds__(kFeatThreads) k_feat(const int* nindex, int n, const int* eweight, int m,
-                                                        FeatAcc* acc, int* sorted) {
+// The 4096-entry hashed weight sample, sorted (a block radix sort, 4 keys per
+// thread) into `sorted`. One CTA of kFeatThreads.
+__device__ __forceinline__ void sort_sample(const int* eweight, int m, int* sorted) {
   typedef cub::BlockRadixSort<int, kFeatThreads, kFeatKeys> SampleSort;
   __shared__ typename SampleSort::TempStorage sort_tmp;
-  __shared__ unsigned long long s[5][32];
-  __shared__ unsigned smax[32];
+  int keys[kFeatKeys];
+#pragma unroll
+  for (int k = 0; k < kFeatKeys; k++) {
+    const int i = threadIdx.x * kFeatKeys + k;
+    const uint64_t r = ecl_mix64(0xFEA70000ull + (uint64_t)i);
+    keys[k] = m > 0 ? __ldg(eweight + (unsigned)(r % (uint64_t)(unsigned)m)) : 0;
+  }
+  SampleSort(sort_tmp).Sort(keys);  // blocked: thread t holds ranks t * kFeatKeys ...
+#pragma unroll
+  for (int k = 0; k < kFeatKeys; k++) sorted[threadIdx.x * kFeatKeys + k] = keys[k];
+}
+
+// The solve's share of the feature pass: the sorted weight sample (the
+// degree statistics come from k_prep).
+__global__ void __launch_bounds__(kFeatThreads) k_sample(const int* eweight, int m, int* sorted) {
+  sort_sample(eweight, m, sorted);
+}
+
+// The whole feature pass for a graph outside a solve: block 0 sorts the
+// weight sample, the other blocks take the degree statistics over all
+// vertices (grid-stride) exactly as k_prep does.
+__global__ void __launch_bounds__(kFeatThreads) k_feat(const int* nindex, int n, const int* eweight, int m,
+                                                        FeatAcc* acc, int* sorted) {
   if (blockIdx.x == 0) {
-    int keys[kFeatKeys];
-#pragma unroll
-    for (int k = 0; k < kFeatKeys; k++) {
-      const int i = threadIdx.x * kFeatKeys + k;
-      const uint64_t r = ecl_mix64(0xFEA70000ull + (uint64_t)i);
-      keys[k] = m > 0 ? __ldg(eweight + (unsigned)(r % (uint64_t)(unsigned)m)) : 0;
-    }
-    SampleSort(sort_tmp).Sort(keys);  // blocked: thread t holds ranks t * kFeatKeys ...
-#pragma unroll
-    for (int k = 0; k < kFeatKeys; k++) sorted[threadIdx.x * kFeatKeys + k] = keys[k];
+    sort_sample(eweight, m, sorted);
     return;
   }
-  unsigned long long d1 = 0, d2 = 0, z = 0, lo = 0, hi = 0;
-  unsigned mx = 0;
+  FeatPart fp;
   const int stride = (gridDim.x - 1) * blockDim.x;
   for (int v = (blockIdx.x - 1) * blockDim.x + threadIdx.x; v < n; v += stride) {
-    const int d = __ldg(nindex + v + 1) - __ldg(nindex + v);
-    const unsigned ud = d > 0 ? (unsigned)d : 0u;
-    d1 += ud;
-    d2 += (unsigned long long)ud * ud;
-    z += ud == 0;
-    lo += ud < 4;
-    hi += ud >= 32;
-    mx = max(mx, ud);
+    const int b = __ldg(nindex + v), e = __ldg(nindex + v + 1);
+    fp.add(e > b ? (unsigned)(e - b) : 0u);
   }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int o = 16; o > 0; o >>= 1) {
-    d1 += __shfl_down_sync(0xffffffffu, d1, o);
-    d2 += __shfl_down_sync(0xffffffffu, d2, o);
-    z += __shfl_down_sync(0xffffffffu, z, o);
-    lo += __shfl_down_sync(0xffffffffu, lo, o);
-    hi += __shfl_down_sync(0xffffffffu, hi, o);
-    mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
-  }
-  if (lane == 0) {
-    s[0][w] = d1;
-    s[1][w] = d2;
-    s[2][w] = z;
-    s[3][w] = lo;
-    s[4][w] = hi;
-    smax[w] = mx;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int i = 1; i < (int)(blockDim.x >> 5); i++) {
-      for (int k = 0; k < 5; k++) s[k][0] += s[k][i];
-      smax[0] = max(smax[0], smax[i]);
-    }
-    atomicAdd(&acc->deg_sum, s[0][0]);
-    atomicAdd(&acc->deg_sq, s[1][0]);
-    atomicAdd(&acc->zero, s[2][0]);
-    atomicAdd(&acc->low, s[3][0]);
-    atomicAdd(&acc->high, s[4][0]);
-    atomicMax(&acc->max_deg, smax[0]);
-  }
+  fp.fold<kFeatThreads>(acc);
 }
 
 // Grid of the feature pass: the sorting block plus up to two degree blocks per SM.
@@ -377,10 +348,6 @@ unsigned ecl_learned_weights_version() {
   return g_w_version;
 }
 
-// Features + MLP on the device for the learned schedule; writes the decoded
-// quantile and split into the solve's control block. Returns
-// ECL_ERR_UNSUPPORTED when no weights are loaded (the caller then falls back
-// to the reference heuristic).
 // Upload the loaded weights to the context's parameter buffer if they
 // changed since its last upload (synchronous: call it outside any stream
 // capture before capturing learned solves).
@@ -402,7 +369,26 @@ int ecl_learned_upload(ecl_mst_ctx* c, cudaStream_t s) {
   return ECL_OK;
 }
 
-int ecl_learned_prepare(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s, void* st) {
+// A learned solve's weight sample, sorted on stream s (after uploading the
+// loaded weights if they changed since this context's last upload).
+int ecl_learned_sample(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s) {
+  int r = ecl_learned_upload(c, s);
+  if (r) return r;
+  float *d_params, *d_feat;
+  void* d_acc;
+  int* d_sample;
+  unsigned* version;
+  int sms = 0;
+  if ((r = ecl_ctx_learned_buffers(c, &d_params, &d_feat, &d_acc, &d_sample, &version, &sms))) return r;
+  k_sample<<<1, kFeatThreads, 0, s>>>(g->eweight, g->edges, d_sample);
+  ML_TRY(cudaGetLastError());
+  return ECL_OK;
+}
+
+// The features (sorted sample + k_prep's degree statistics) and the MLP, on
+// stream s once both are complete; writes the decoded schedule into the
+// solve's control block `st`.
+int ecl_learned_apply(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s, void* st) {
   float *d_params, *d_feat;
   void* d_acc;
   int* d_sample;
@@ -410,18 +396,6 @@ int ecl_learned_prepare(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s, void
   int sms = 0;
   int r = ecl_ctx_learned_buffers(c, &d_params, &d_feat, &d_acc, &d_sample, &version, &sms);
   if (r) return r;
-  {
-    std::lock_guard<std::mutex> lock(g_w_mu);
-    if (g_weights.empty()) return ECL_ERR_UNSUPPORTED;
-    if (*version != g_w_version) {  // upload only when the loaded weights changed
-      ML_TRY(cudaMemcpyAsync(d_params, g_weights.data(), kParams * sizeof(float), cudaMemcpyHostToDevice, s));
-      ML_TRY(cudaStreamSynchronize(s));
-      *version = g_w_version;
-    }
-  }
-  ML_TRY(cudaMemsetAsync(d_acc, 0, sizeof(FeatAcc), s));
-  k_feat<<<feat_grid(g->nodes, sms), kFeatThreads, 0, s>>>(g->nindex, g->nodes, g->eweight, g->edges,
-                                                          (FeatAcc*)d_acc, d_sample);
   k_mlp_apply<<<1, 256, 0, s>>>(d_params, (const FeatAcc*)d_acc, d_sample, g->nodes, g->edges,
                                (ecl::DevState*)st);
   ML_TRY(cudaGetLastError());

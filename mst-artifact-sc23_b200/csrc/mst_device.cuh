@@ -75,6 +75,12 @@ constexpr int kSplitAfter = 8;         // find steps before path splitting start
 #ifndef ECL_L2_HINTS
 #define ECL_L2_HINTS 1                 // evict-first CSR streams, evict-last parent gathers in the scans
 #endif
+// How the heavy scan gathers parent[] under the L2 policies (parent[] is
+// read-only for the whole launch): 0 = through L2 only, 1 = through L1 as
+// well (non-coherent loads).
+#ifndef ECL_SCAN_GATHER_L1
+#define ECL_SCAN_GATHER_L1 0
+#endif
 constexpr unsigned long long kBarrierTimeoutNs = 5ull * 1000 * 1000 * 1000;
 
 // Entries per thread of the edge-balanced scan for a degree split: rows
@@ -95,6 +101,7 @@ struct PrepArgs {
   int mode, explicit_thr, split;
   float quantile;
   DevState* st;
+  FeatAcc* feat;  // learned schedule: degree statistics gathered here, else null
 };
 
 struct ScanArgs {
@@ -254,6 +261,7 @@ __global__ void __launch_bounds__(kThreads) k_prep(PrepArgs a) {
   const int n = a.nodes, m = a.edges;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   bool bad = false;
+  FeatPart fp;  // degree statistics (learned schedule)
   for (int v = gid; v < n; v += stride) {
     a.parent[v] = v;
     a.minv0[v] = kNoEdge;
@@ -261,6 +269,7 @@ __global__ void __launch_bounds__(kThreads) k_prep(PrepArgs a) {
     const int b = __ldg(a.nindex + v), e = __ldg(a.nindex + v + 1);
     const bool row_bad = b < 0 || e < b || e > m;
     bad |= row_bad;
+    if (a.feat) fp.add(e > b ? (unsigned)(e - b) : 0u);
     // Tile->vertex table (first_v[t] = row of entry t * kGran), first step:
     // the row holding the first step position at or after its start writes
     // itself there (each position has exactly one owner, so no conflicts);
@@ -271,6 +280,7 @@ __global__ void __launch_bounds__(kThreads) k_prep(PrepArgs a) {
   }
   if (gid == 0) bad |= __ldg(a.nindex) != 0 || __ldg(a.nindex + n) != m;
   if (bad) atomicOr(&st->error, kErrFormat);
+  if (a.feat) fp.fold<kThreads>(a.feat);  // uniform across the grid
 }
 
 // Inclusive max scan of the tile->vertex table first_v[0 .. tiles), in
@@ -522,6 +532,12 @@ __device__ void scan_produce(const ScanArgs& a, unsigned char* smem, int ntiles)
         atomicOr(&a.st->error, kErrTimeout);
 }
 
+// One parent[] gather of the heavy scan.
+__device__ __forceinline__ int gather_parent(const int* p, u64 policy) {
+  if (!ECL_L2_HINTS) return __ldg(p);
+  return ECL_SCAN_GATHER_L1 ? ld_nc_hint(p, policy) : ld_cg_hint(p, policy);
+}
+
 template <int KIND, int EPT>
 __global__ void __launch_bounds__(kScanThreads, ScanCfg<EPT>::kMinBlocks) k_scan(ScanArgs a) {
   using C = ScanCfg<EPT>;
@@ -672,10 +688,10 @@ __global__ void __launch_bounds__(kScanThreads, ScanCfg<EPT>::kMinBlocks) k_scan
         if (cand & (1u << q)) {
           if (vtx[q] != rv) {
             rv = vtx[q];
-            rrep = ECL_L2_HINTS ? ld_cg_hint(a.parent + rv, keep_pol) : __ldg(a.parent + rv);
+            rrep = gather_parent(a.parent + rv, keep_pol);
           }
           vtx[q] = rrep;
-          nrep[q] = ECL_L2_HINTS ? ld_cg_hint(a.parent + nb[q], keep_pol) : __ldg(a.parent + nb[q]);
+          nrep[q] = gather_parent(a.parent + nb[q], keep_pol);
         }
 #pragma unroll
       for (int q = 0; q < EPT; q++)

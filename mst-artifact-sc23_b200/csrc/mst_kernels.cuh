@@ -28,6 +28,66 @@ constexpr int kChunkLog = 7;  // long rows are scanned in aligned 128-entry chun
 constexpr int kChunk = 1 << kChunkLog;
 constexpr u64 kNoEdge = ~0ull;
 
+// Degree statistics of the learned schedule's features, summed over all
+// vertices (row degree = nindex[v + 1] - nindex[v]).
+struct FeatAcc {
+  unsigned long long deg_sum, deg_sq, zero, low, high;  // sum d, sum d^2, #d = 0, #d < 4, #d >= 32
+  unsigned max_deg;
+};
+
+// One thread's part of the degree statistics.
+struct FeatPart {
+  unsigned long long d1 = 0, d2 = 0, z = 0, lo = 0, hi = 0;
+  unsigned mx = 0;
+  __device__ __forceinline__ void add(unsigned d) {
+    d1 += d;
+    d2 += (unsigned long long)d * d;
+    z += d == 0;
+    lo += d < 4;
+    hi += d >= 32;
+    mx = max(mx, d);
+  }
+  // Fold the CTA's parts into `acc`: warp shuffles, one shared-memory pass,
+  // one atomic per counter per CTA. Every thread of the CTA (kBlock threads)
+  // must call this.
+  template <int kBlock>
+  __device__ __forceinline__ void fold(FeatAcc* acc) {
+    __shared__ unsigned long long part[5][kBlock / 32];
+    __shared__ unsigned pmax[kBlock / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      d1 += __shfl_down_sync(0xffffffffu, d1, o);
+      d2 += __shfl_down_sync(0xffffffffu, d2, o);
+      z += __shfl_down_sync(0xffffffffu, z, o);
+      lo += __shfl_down_sync(0xffffffffu, lo, o);
+      hi += __shfl_down_sync(0xffffffffu, hi, o);
+      mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    }
+    if (lane == 0) {
+      part[0][w] = d1;
+      part[1][w] = d2;
+      part[2][w] = z;
+      part[3][w] = lo;
+      part[4][w] = hi;
+      pmax[w] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int i = 1; i < kBlock / 32; i++) {
+        for (int k = 0; k < 5; k++) part[k][0] += part[k][i];
+        pmax[0] = max(pmax[0], pmax[i]);
+      }
+      atomicAdd(&acc->deg_sum, part[0][0]);
+      atomicAdd(&acc->deg_sq, part[1][0]);
+      atomicAdd(&acc->zero, part[2][0]);
+      atomicAdd(&acc->low, part[3][0]);
+      atomicAdd(&acc->high, part[4][0]);
+      atomicMax(&acc->max_deg, pmax[0]);
+    }
+  }
+};
+
 // Control block of one solve, zeroed before every solve.
 struct DevState {
   int threshold;       // light phase keeps w <= threshold
@@ -193,6 +253,14 @@ __device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, unsign
 __device__ __forceinline__ int ld_cg_hint(const int* p, u64 policy) {
   int v;
   asm volatile("ld.global.cg.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy));
+  return v;
+}
+
+// 32-bit read-only global load (non-coherent path, L1 allocating) with an L2
+// cache policy; only for data no thread writes during the launch.
+__device__ __forceinline__ int ld_nc_hint(const int* p, u64 policy) {
+  int v;
+  asm volatile("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy));
   return v;
 }
 
