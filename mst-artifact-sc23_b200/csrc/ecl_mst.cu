@@ -42,9 +42,12 @@ struct ecl_mst_ctx {
   int sm_count = 0;
   int64_t max_nodes = 0, max_edges = 0;
   cudaStream_t stream = nullptr;
-  // the learned schedule's feature pass runs on `side`, beside k_prep
-  cudaStream_t side = nullptr;
+  // the learned schedule's sample sort and MLP run on `side`, beside k_prep
+  // and the fill scan; the scan variants its split does not select run on
+  // `side` and `side2`, beside the selected one
+  cudaStream_t side = nullptr, side2 = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr, prep_done = nullptr;
+  cudaEvent_t scan_fork = nullptr, scan_join[2] = {nullptr, nullptr};
   // the last solve's key, and the captured solve (CUDA graph) with its key
   std::vector<long long> last_key, exec_key;
   cudaGraphExec_t exec = nullptr;
@@ -300,6 +303,10 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   if ((st = cuda_status(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming)))) return fail(st);
   if ((st = cuda_status(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming)))) return fail(st);
   if ((st = cuda_status(cudaEventCreateWithFlags(&c->prep_done, cudaEventDisableTiming)))) return fail(st);
+  if ((st = cuda_status(cudaStreamCreateWithFlags(&c->side2, cudaStreamNonBlocking)))) return fail(st);
+  if ((st = cuda_status(cudaEventCreateWithFlags(&c->scan_fork, cudaEventDisableTiming)))) return fail(st);
+  for (auto& e : c->scan_join)
+    if ((st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)))) return fail(st);
   const size_t slot_bytes = (size_t)max_nodes * (2 * sizeof(u64) + sizeof(int));
   if ((st = cuda_status(cudaMalloc(&c->slots, slot_bytes)))) return fail(st);
   c->l2_persist_max = prop.persistingL2CacheMaxSize > 0 ? (size_t)prop.persistingL2CacheMaxSize : 0;
@@ -363,10 +370,15 @@ extern "C" void ecl_mst_ctx_destroy(ecl_mst_ctx* c) {
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->side) cudaStreamSynchronize(c->side);
+  if (c->side2) cudaStreamSynchronize(c->side2);
   if (c->exec) cudaGraphExecDestroy(c->exec);
   if (c->fork) cudaEventDestroy(c->fork);
   if (c->join) cudaEventDestroy(c->join);
   if (c->prep_done) cudaEventDestroy(c->prep_done);
+  if (c->scan_fork) cudaEventDestroy(c->scan_fork);
+  for (cudaEvent_t e : c->scan_join)
+    if (e) cudaEventDestroy(e);
+  if (c->side2) cudaStreamDestroy(c->side2);
   if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -459,13 +471,23 @@ int launch_scan(int ept, const ScanArgs& sa, cudaStream_t s, const cudaAccessPol
 
 // Scan variants to launch: the one the split selects, or all three (each
 // exits unless st->split selects it) when the split is chosen on the device.
+// Those three go on forked streams, so the two that exit at once do so beside
+// the selected one instead of after it.
 template <int KIND>
-int launch_scans(bool device_split, int split, const ScanArgs& sa, cudaStream_t s,
+int launch_scans(ecl_mst_ctx* c, bool device_split, int split, const ScanArgs& sa, cudaStream_t s,
                  const cudaAccessPolicyWindow* win) {
   if (!device_split) return launch_scan<KIND>(scan_ept(split), sa, s, win);
+  const cudaStream_t br[2] = {c->side, c->side2};
+  ECL_CUDA_TRY(cudaEventRecord(c->scan_fork, s));
+  for (cudaStream_t b : br) ECL_CUDA_TRY(cudaStreamWaitEvent(b, c->scan_fork, 0));
   int st;
-  for (int ept : {4, 8, 16})
-    if ((st = launch_scan<KIND>(ept, sa, s, win))) return st;
+  if ((st = launch_scan<KIND>(8, sa, s, win))) return st;  // the split the network picks most often
+  if ((st = launch_scan<KIND>(4, sa, br[0], win))) return st;
+  if ((st = launch_scan<KIND>(16, sa, br[1], win))) return st;
+  for (int i = 0; i < 2; i++) {
+    ECL_CUDA_TRY(cudaEventRecord(c->scan_join[i], br[i]));
+    ECL_CUDA_TRY(cudaStreamWaitEvent(s, c->scan_join[i], 0));
+  }
   return ECL_OK;
 }
 
@@ -622,7 +644,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
     return ECL_OK;
   }
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[5], s));
-  if ((st = launch_scans<kLight>(device_split, split, sa, s, nullptr))) return st;
+  if ((st = launch_scans<kLight>(c, device_split, split, sa, s, nullptr))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   ra.phase = 0;
   if (win_all) st = launch_ex(k_rounds, rgrid, kRoundThreads, 0, s, true, win_all, ra);
@@ -639,7 +661,7 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
     ECL_CUDA_TRY(cudaGetLastError());
   }
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[6], s));
-  if ((st = launch_scans<kHeavy>(device_split, split, sa, s, win_par))) return st;
+  if ((st = launch_scans<kHeavy>(c, device_split, split, sa, s, win_par))) return st;
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[3], s));
   ra.phase = 1;
   if (win_all) st = launch_ex(k_rounds, rgrid, kRoundThreads, 0, s, true, win_all, ra);

@@ -75,12 +75,6 @@ constexpr int kSplitAfter = 8;         // find steps before path splitting start
 #ifndef ECL_L2_HINTS
 #define ECL_L2_HINTS 1                 // evict-first CSR streams, evict-last parent gathers in the scans
 #endif
-// How the heavy scan gathers parent[] under the L2 policies (parent[] is
-// read-only for the whole launch): 0 = through L2 only, 1 = through L1 as
-// well (non-coherent loads).
-#ifndef ECL_SCAN_GATHER_L1
-#define ECL_SCAN_GATHER_L1 0
-#endif
 constexpr unsigned long long kBarrierTimeoutNs = 5ull * 1000 * 1000 * 1000;
 
 // Entries per thread of the edge-balanced scan for a degree split: rows
@@ -532,10 +526,11 @@ __device__ void scan_produce(const ScanArgs& a, unsigned char* smem, int ntiles)
         atomicOr(&a.st->error, kErrTimeout);
 }
 
-// One parent[] gather of the heavy scan.
+// One parent[] gather of the heavy scan, through L2 with the evict-last
+// policy (L1-allocating loads measured no faster: the gathers rarely repeat
+// within an SM).
 __device__ __forceinline__ int gather_parent(const int* p, u64 policy) {
-  if (!ECL_L2_HINTS) return __ldg(p);
-  return ECL_SCAN_GATHER_L1 ? ld_nc_hint(p, policy) : ld_cg_hint(p, policy);
+  return ECL_L2_HINTS ? ld_cg_hint(p, policy) : __ldg(p);
 }
 
 template <int KIND, int EPT>

@@ -256,14 +256,6 @@ __device__ __forceinline__ int ld_cg_hint(const int* p, u64 policy) {
   return v;
 }
 
-// 32-bit read-only global load (non-coherent path, L1 allocating) with an L2
-// cache policy; only for data no thread writes during the launch.
-__device__ __forceinline__ int ld_nc_hint(const int* p, u64 policy) {
-  int v;
-  asm volatile("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy));
-  return v;
-}
-
 // Shared memory of one CTA-wide two-counter reservation.
 struct ReserveSmem {
   unsigned warp_off[32][2];

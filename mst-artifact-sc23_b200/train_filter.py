@@ -24,7 +24,7 @@
    tables.
 
     python train_filter.py --train 3000 --heldout 500 --out-dir <dir> --dataset <sweeps.npz>
-    python train_filter.py --eval-only <sweeps.npz> --weights <blob> --out-dir <dir>
+    python train_filter.py --eval-only <sweeps.npz> [<large.npz>] --weights <blob> --out-dir <dir>
     python train_filter.py --nmin 4000000 --nmax 33554432 --seed-offset 50000 \
         --train 500 --heldout 150 --out-dir <dir> --dataset <large.npz>
     python train_filter.py --from-datasets <sweeps.npz> <large.npz> --out-dir <dir>
@@ -202,7 +202,7 @@ def run(args):
     summary_extra = {}
     parts = None
     if args.eval_only or args.from_datasets:
-        parts = [load_dataset(d) for d in (args.from_datasets or [args.eval_only])]
+        parts = [load_dataset(d) for d in (args.from_datasets or args.eval_only)]
         args.nmin = min(min(h["nmin"]) for _, h in parts)
         args.nmax = max(max(h["nmax"]) for _, h in parts)
     # largest graphs drawn: RMAT scale 22 at edge factor 32 and ER n_max at degree
@@ -226,6 +226,8 @@ def run(args):
         else:
             p, hist = train_on(tr, args.seed, args.epochs, args.lr)
             summary_extra["datasets"] = [os.path.basename(d) for d in args.from_datasets]
+        if args.eval_only:
+            summary_extra["datasets"] = [os.path.basename(d) for d in args.eval_only]
         args.train, args.heldout = len(tr["x"]), len(ho["x"])
     else:
         t0 = time.time()
@@ -325,7 +327,7 @@ if __name__ == "__main__":
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out-dir", default=HERE)
     ap.add_argument("--dataset", default=None, help="also write the sweep tables (.npz) here")
-    ap.add_argument("--eval-only", default=None, metavar="DATASET",
+    ap.add_argument("--eval-only", nargs="+", default=None, metavar="DATASET",
                     help="evaluate --weights on these saved sweep tables and measure the held-out graphs again")
     ap.add_argument("--weights", default=os.path.join(HERE, "filter_weights.bin"))
     ap.add_argument("--from-datasets", nargs="+", default=None, metavar="DATASET",
