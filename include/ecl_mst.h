@@ -484,6 +484,13 @@ void* ecl_mst_ctx_stream(ecl_mst_ctx* ctx);
  * no L2 policy. */
 int ecl_mst_ctx_l2_reset(ecl_mst_ctx* ctx);
 
+/* The 16 features the last learned-schedule solve on this context fed its
+ * network (the degree statistics k_prep gathered and the sorted weight
+ * sample), copied to host out16 after the context's streams finish; they
+ * equal ecl_graph_features() of the same graph. ECL_ERR_UNSUPPORTED before
+ * any learned solve on the context. No counterpart in the reference. */
+int ecl_mst_ctx_learned_features(ecl_mst_ctx* ctx, float* out16);
+
 /* Pinned host memory for fast H2D/D2H (cudaHostAlloc / cudaFreeHost). */
 int ecl_host_alloc_pinned(size_t bytes, void** out);
 void ecl_host_free_pinned(void* p);

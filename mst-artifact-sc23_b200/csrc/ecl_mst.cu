@@ -117,7 +117,8 @@ struct ecl_mst_ctx {
   // features, degree accumulators, the sorted 4096-entry weight sample
   float* ml_params = nullptr;
   unsigned ml_version = ~0u;
-  float* ml_feat = nullptr;
+  float* ml_feat = nullptr;  // the features of the last learned solve
+  bool ml_features_set = false;
   void* ml_acc = nullptr;
   int* ml_sample = nullptr;
 };
@@ -386,6 +387,15 @@ extern "C" void ecl_mst_ctx_destroy(ecl_mst_ctx* c) {
 
 extern "C" void* ecl_mst_ctx_stream(ecl_mst_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
+extern "C" int ecl_mst_ctx_learned_features(ecl_mst_ctx* c, float* out16) {
+  if (!c || !out16) return ECL_ERR_INVALID_ARG;
+  if (!c->ml_features_set) return ECL_ERR_UNSUPPORTED;
+  ECL_CUDA_TRY(cudaSetDevice(c->device));
+  ECL_CUDA_TRY(cudaStreamSynchronize(c->side));
+  ECL_CUDA_TRY(cudaMemcpy(out16, c->ml_feat, ECL_MLP_INPUTS * sizeof(float), cudaMemcpyDeviceToHost));
+  return ECL_OK;
+}
+
 extern "C" int ecl_mst_ctx_l2_reset(ecl_mst_ctx* c) {
   if (!c) return ECL_ERR_INVALID_ARG;
   ECL_CUDA_TRY(cudaSetDevice(c->device));
@@ -526,6 +536,7 @@ struct LearnedPlan {
 // there. Fills lp->acc.
 int learned_fork(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t q, LearnedPlan* lp) {
   lp->acc = static_cast<FeatAcc*>(c->ml_acc);
+  c->ml_features_set = true;
   ECL_CUDA_TRY(cudaMemsetAsync(lp->acc, 0, sizeof(FeatAcc), q));
   ECL_CUDA_TRY(cudaEventRecord(c->fork, q));
   ECL_CUDA_TRY(cudaStreamWaitEvent(lp->side, c->fork, 0));

@@ -173,7 +173,7 @@ __host__ __device__ __forceinline__ float heuristic_log2_quantile(int n, int m) 
 // decoded quantile selects the light-phase threshold from the sorted weight
 // sample of the feature pass.
 __global__ void k_mlp_apply(const float* pg, const FeatAcc* acc, const int* sorted, int n, int m,
-                            ecl::DevState* st) {
+                            ecl::DevState* st, float* feat_out) {
   // the whole parameter blob (21 KB) is staged in shared memory first, so the
   // layers read it at shared-memory latency instead of one global load per
   // multiply-add
@@ -183,7 +183,10 @@ __global__ void k_mlp_apply(const float* pg, const FeatAcc* acc, const int* sort
   for (int i = j; i < kParams; i += blockDim.x) p[i] = __ldg(pg + i);
   if (j == 0) compute_features(n, m, acc, sorted, fx);
   __syncthreads();
-  if (j < kIn) xs[j] = (fx[j] - p[kOffMean + j]) / p[kOffStd + j];
+  if (j < kIn) {
+    feat_out[j] = fx[j];  // kept for ecl_mst_ctx_learned_features
+    xs[j] = (fx[j] - p[kOffMean + j]) / p[kOffStd + j];
+  }
   __syncthreads();
   if (j < kH) {
     float a = p[kOffB1 + j];
@@ -397,7 +400,7 @@ int ecl_learned_apply(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s, void* 
   int r = ecl_ctx_learned_buffers(c, &d_params, &d_feat, &d_acc, &d_sample, &version, &sms);
   if (r) return r;
   k_mlp_apply<<<1, 256, 0, s>>>(d_params, (const FeatAcc*)d_acc, d_sample, g->nodes, g->edges,
-                               (ecl::DevState*)st);
+                               (ecl::DevState*)st, d_feat);
   ML_TRY(cudaGetLastError());
   return ECL_OK;
 }

@@ -130,6 +130,7 @@ def load():
         "ecl_mst_run_device_noalloc": (c_int, [G, c_void_p, POINTER(MstOpts), c_void_p]),
         "ecl_mst_ctx_stream": (c_void_p, [c_void_p]),
         "ecl_mst_ctx_l2_reset": (c_int, [c_void_p]),
+        "ecl_mst_ctx_learned_features": (c_int, [c_void_p, c_void_p]),
         "ecl_mst_ctx_run_host_async": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
         "ecl_mst_ctx_wait": (c_int, [c_void_p]),
         "ecl_host_alloc_pinned": (c_int, [ctypes.c_size_t, POINTER(c_void_p)]),
@@ -558,6 +559,12 @@ class Context:
     def l2_reset(self):
         """Return L2 lines marked persisting (FLAG_L2_PERSIST) to normal."""
         _check(self._lib.ecl_mst_ctx_l2_reset(self.handle), "ctx_l2_reset")
+
+    def learned_features(self):
+        """The 16 features the last learned-schedule solve fed its network."""
+        out = np.zeros(MLP_IN, np.float32)
+        _check(self._lib.ecl_mst_ctx_learned_features(self.handle, _ptr(out)), "ctx_learned_features")
+        return out
 
 
 class Batch:

@@ -88,6 +88,34 @@ def test_device_features_match_host_statistics():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("family", ["grid", "er", "rmat", "rgg"])
+def test_solve_features_equal_the_feature_pass(family):
+    """A learned solve takes its degree statistics from k_prep's vertex pass
+    and sorts the weight sample beside it; the features it feeds the network
+    are bit for bit those of the standalone feature pass (ecl_graph_features)
+    that the training sweeps record."""
+    import torch
+    if not E.learned_load_default():
+        pytest.skip("no trained weights shipped")
+    dg = {"grid": lambda: E.gen_grid_device(700, 700, 3, 1 << 20),
+          "er": lambda: E.gen_er_device(100_000, 16.0, 3, 1 << 24),
+          "rmat": lambda: E.gen_rmat_device(17, 16, 0.57, 0.19, 0.19, 3, 1 << 30),
+          "rgg": lambda: E.gen_rgg2d_device(400_000, 3.0, 3, 1 << 24)}[family]()
+    assert dg.edges >= 1 << 20  # graphs below that keep the heuristic
+    out = torch.empty(dg.edges, dtype=torch.uint8, device="cuda:0")
+    want = E.graph_features(dg.nodes, dg.edges, dg.d_nindex, dg.d_nlist, dg.d_eweight)
+    with E.Context(dg.nodes, dg.edges) as ctx:
+        with pytest.raises(E.EclError):
+            ctx.learned_features()  # no learned solve yet
+        st = ctx.run_device(dg.nodes, dg.edges, dg.d_nindex, dg.d_nlist, dg.d_eweight, out.data_ptr(),
+                            opts=E.make_opts(mode=E.THRESH_LEARNED), stats=True)
+        assert st["status"] == 0
+        got = ctx.learned_features()
+    dg.close()
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.gpu
 def test_learned_mode_keeps_the_answer(golden):
     rng = np.random.default_rng(8)
     p = E.mlp_init(9, mean=np.zeros(16), std=np.ones(16))
