@@ -14,11 +14,15 @@
 #include "internal.h"
 #include "mst_device.cuh"
 #include "batch_device.cuh"
+#include <functional>
 #include <vector>
 
-// Learned schedule weights (learned.cu): the context's device copy of the
-// loaded parameter blob is refreshed when the loaded weights changed (the
-// network itself runs inside k_prep).
+// Learned threshold/split (learned.cu). ecl_learned_sample uploads changed
+// weights and sorts the weight sample; ecl_learned_apply computes the
+// features from it and from k_prep's degree statistics and runs the trained
+// MLP, writing DevState::threshold, filtered, quantile and split.
+int ecl_learned_sample(ecl_mst_ctx* c, const ecl_graph* d_graph, cudaStream_t s);
+int ecl_learned_apply(ecl_mst_ctx* c, const ecl_graph* d_graph, cudaStream_t s, void* st);
 int ecl_learned_upload(ecl_mst_ctx* c, cudaStream_t s);
 unsigned ecl_learned_weights_version();
 
@@ -38,9 +42,11 @@ struct ecl_mst_ctx {
   int sm_count = 0;
   int64_t max_nodes = 0, max_edges = 0;
   cudaStream_t stream = nullptr;
-  // the scan variants the learned schedule's split does not select run on
+  // the learned schedule's sample sort and MLP run on `side`, beside k_prep
+  // and the fill scan; the scan variants its split does not select run on
   // `side` and `side2`, beside the selected one
   cudaStream_t side = nullptr, side2 = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr, prep_done = nullptr;
   cudaEvent_t scan_fork = nullptr, scan_join[2] = {nullptr, nullptr};
   // the last solve's key, and the captured solve (CUDA graph) with its key
   std::vector<long long> last_key, exec_key;
@@ -113,7 +119,8 @@ struct ecl_mst_ctx {
   unsigned ml_version = ~0u;
   float* ml_feat = nullptr;  // the features of the last learned solve
   bool ml_features_set = false;
-  int* ml_sample = nullptr;  // its sorted weight sample
+  void* ml_acc = nullptr;
+  int* ml_sample = nullptr;
 };
 
 namespace {
@@ -201,8 +208,11 @@ int64_t first_v_entries(int64_t edges) {
 
 // k_prep, then the fill scan that completes the tile->vertex table
 // (first_v: pa.tiles + 1 entries, then room for the chunk maxima).
-// k_prep, then the max scan of the tile->vertex table.
-int enqueue_prep(const PrepArgs& pa, int sm_count, cudaStream_t s, const cudaAccessPolicyWindow* win = nullptr) {
+// k_prep, then the max scan of the tile->vertex table. `after_prep`, when
+// given, is enqueued between the two (the learned schedule forks its MLP off
+// there, once k_prep's degree statistics are complete).
+int enqueue_prep(const PrepArgs& pa, int sm_count, cudaStream_t s, const cudaAccessPolicyWindow* win = nullptr,
+                 const std::function<int()>& after_prep = nullptr) {
   ECL_CUDA_TRY(cudaMemsetAsync(pa.first_v, 0, sizeof(int) * (size_t)pa.tiles, s));
   const int prep_grid = (int)std::min<int64_t>((pa.nodes + kThreads - 1) / kThreads, (int64_t)sm_count * 16);
   if (win) {
@@ -212,6 +222,10 @@ int enqueue_prep(const PrepArgs& pa, int sm_count, cudaStream_t s, const cudaAcc
     k_prep<<<std::max(prep_grid, 1), kThreads, 0, s>>>(pa);
   }
   ECL_CUDA_TRY(cudaGetLastError());
+  if (after_prep) {
+    const int st = after_prep();
+    if (st) return st;
+  }
   const int chunks = (pa.tiles + kFillChunk - 1) / kFillChunk;
   int* chunk_max = pa.first_v + pa.tiles + 1;
   k_fill_chunks<<<chunks, 1024, 0, s>>>(pa.first_v, pa.tiles, chunk_max);
@@ -287,6 +301,9 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   c->sm_count = prop.multiProcessorCount;
   if ((st = cuda_status(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)))) return fail(st);
   if ((st = cuda_status(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)))) return fail(st);
+  if ((st = cuda_status(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming)))) return fail(st);
+  if ((st = cuda_status(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming)))) return fail(st);
+  if ((st = cuda_status(cudaEventCreateWithFlags(&c->prep_done, cudaEventDisableTiming)))) return fail(st);
   if ((st = cuda_status(cudaStreamCreateWithFlags(&c->side2, cudaStreamNonBlocking)))) return fail(st);
   if ((st = cuda_status(cudaEventCreateWithFlags(&c->scan_fork, cudaEventDisableTiming)))) return fail(st);
   for (auto& e : c->scan_join)
@@ -301,6 +318,7 @@ extern "C" int ecl_mst_ctx_create(int device, int64_t max_nodes, int64_t max_edg
   if ((st = cuda_status(cudaMalloc(&c->st, sizeof(DevState))))) return fail(st);
   if ((st = cuda_status(cudaMalloc(&c->ml_params, ECL_MLP_PARAMS * sizeof(float))))) return fail(st);
   if ((st = cuda_status(cudaMalloc(&c->ml_feat, ECL_MLP_INPUTS * sizeof(float))))) return fail(st);
+  if ((st = cuda_status(cudaMalloc(&c->ml_acc, sizeof(FeatAcc))))) return fail(st);
   if ((st = cuda_status(cudaMalloc(&c->ml_sample, 4096 * sizeof(int))))) return fail(st);
   if ((st = cuda_status(cudaHostAlloc(&c->st_host, sizeof(DevState), cudaHostAllocDefault))))
     return fail(st);
@@ -330,6 +348,7 @@ extern "C" void ecl_mst_ctx_destroy(ecl_mst_ctx* c) {
   cudaFree(c->slist);
   cudaFree(c->ml_params);
   cudaFree(c->ml_feat);
+  cudaFree(c->ml_acc);
   cudaFree(c->ml_sample);
   cudaFree(c->st);
   cudaFreeHost(c->st_host);
@@ -354,6 +373,9 @@ extern "C" void ecl_mst_ctx_destroy(ecl_mst_ctx* c) {
   if (c->side) cudaStreamSynchronize(c->side);
   if (c->side2) cudaStreamSynchronize(c->side2);
   if (c->exec) cudaGraphExecDestroy(c->exec);
+  if (c->fork) cudaEventDestroy(c->fork);
+  if (c->join) cudaEventDestroy(c->join);
+  if (c->prep_done) cudaEventDestroy(c->prep_done);
   if (c->scan_fork) cudaEventDestroy(c->scan_fork);
   for (cudaEvent_t e : c->scan_join)
     if (e) cudaEventDestroy(e);
@@ -369,7 +391,7 @@ extern "C" int ecl_mst_ctx_learned_features(ecl_mst_ctx* c, float* out16) {
   if (!c || !out16) return ECL_ERR_INVALID_ARG;
   if (!c->ml_features_set) return ECL_ERR_UNSUPPORTED;
   ECL_CUDA_TRY(cudaSetDevice(c->device));
-  ECL_CUDA_TRY(cudaDeviceSynchronize());  // the solve may have run on any stream
+  ECL_CUDA_TRY(cudaStreamSynchronize(c->side));
   ECL_CUDA_TRY(cudaMemcpy(out16, c->ml_feat, ECL_MLP_INPUTS * sizeof(float), cudaMemcpyDeviceToHost));
   return ECL_OK;
 }
@@ -499,13 +521,30 @@ bool l2_window(const ecl_mst_ctx* c, const Slots& sl, bool parent_only, cudaAcce
   return true;
 }
 
-// One solve on stream s. In learned mode k_prep also runs the network: its
-// block 0 sorts the weight sample, every CTA sums the degree statistics of
-// its vertices, and the CTA that finishes last computes the features and
-// decides the threshold and split (the context's parameter copy must be
-// current: ecl_learned_upload).
+// The learned schedule's steps around k_prep. The weight sample is sorted on
+// `side` from the start of the solve (ecl_learned_sample); k_prep gathers the
+// degree statistics into `acc` on the solve's stream; the MLP then runs on
+// `side` beside the fill scan, and the light scan waits for it.
+struct LearnedPlan {
+  cudaStream_t side;
+  cudaEvent_t prep_done, join;
+  FeatAcc* acc;
+};
+
+// Start of a learned solve on stream q: zero the degree accumulator (before
+// k_prep adds to it), then fork the side stream and sort the weight sample
+// there. Fills lp->acc.
+int learned_fork(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t q, LearnedPlan* lp) {
+  lp->acc = static_cast<FeatAcc*>(c->ml_acc);
+  c->ml_features_set = true;
+  ECL_CUDA_TRY(cudaMemsetAsync(lp->acc, 0, sizeof(FeatAcc), q));
+  ECL_CUDA_TRY(cudaEventRecord(c->fork, q));
+  ECL_CUDA_TRY(cudaStreamWaitEvent(lp->side, c->fork, 0));
+  return ecl_learned_sample(c, g, lp->side);
+}
+
 int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, const mst_opts* o,
-                  cudaStream_t s, bool timed) {
+                  cudaStream_t s, bool timed, const LearnedPlan* lp = nullptr) {
   const int n = g->nodes, m = g->edges;
   const int split = o->degree_split > 0 ? o->degree_split : kDefaultSplit;
   const bool device_split = o->threshold_mode == ECL_THRESH_LEARNED;
@@ -532,14 +571,20 @@ int enqueue_solve(ecl_mst_ctx* c, const ecl_graph* g, unsigned char* d_inMST, co
   pa.split = split;
   pa.quantile = o->quantile;
   pa.st = c->st;
-  if (device_split) {
-    pa.mlp = c->ml_params;
-    pa.sample = c->ml_sample;
-    pa.feat_out = c->ml_feat;
-    c->ml_features_set = true;
-  }
+  pa.feat = lp ? lp->acc : nullptr;
   int st;
-  if ((st = enqueue_prep(pa, c->sm_count, s, win_all))) return st;
+  std::function<int()> fork_mlp;
+  if (lp)
+    fork_mlp = [&]() -> int {
+      ECL_CUDA_TRY(cudaEventRecord(lp->prep_done, s));
+      ECL_CUDA_TRY(cudaStreamWaitEvent(lp->side, lp->prep_done, 0));
+      const int r = ecl_learned_apply(c, g, lp->side, c->st);
+      if (r) return r;
+      ECL_CUDA_TRY(cudaEventRecord(lp->join, lp->side));
+      return ECL_OK;
+    };
+  if ((st = enqueue_prep(pa, c->sm_count, s, win_all, fork_mlp))) return st;
+  if (lp) ECL_CUDA_TRY(cudaStreamWaitEvent(s, lp->join, 0));
   const bool no_tuples = (o->flags & (ECL_FLAG_NO_TUPLES | ECL_FLAG_NO_EDGE_BASED)) == ECL_FLAG_NO_TUPLES;
   if (no_tuples) {  // the vertex of every entry, for the gathers of the rounds
     const int sgrid = (int)std::min<int64_t>(((int64_t)m + kThreads - 1) / kThreads, (int64_t)c->sm_count * 16);
@@ -709,9 +754,14 @@ int check_opts(const mst_opts* o) {
 
 }  // namespace
 
-int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, unsigned** version) {
+int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, float** feat, void** acc, int** sample,
+                            unsigned** version, int* sm_count) {
+  *sample = c->ml_sample;
   *version = &c->ml_version;
   *params = c->ml_params;
+  *feat = c->ml_feat;
+  *acc = c->ml_acc;
+  *sm_count = c->sm_count;
   return ECL_OK;
 }
 
@@ -758,11 +808,10 @@ int run_device_once(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d_inMST, const 
     ECL_CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevState), q));
     // the timed window starts before the learned schedule's feature pass
     if (inner_events) ECL_CUDA_TRY(cudaEventRecord(c->ev[0], q));
-    if (o.threshold_mode == ECL_THRESH_LEARNED) {
-      const int r = ecl_learned_upload(c, q);  // a no-op unless the loaded weights changed
-      if (r) return r;
-    }
-    return enqueue_solve(c, g, d_inMST, &o, q, inner_events);
+    if (o.threshold_mode != ECL_THRESH_LEARNED) return enqueue_solve(c, g, d_inMST, &o, q, inner_events);
+    LearnedPlan lp{c->side, c->prep_done, c->join, nullptr};
+    const int r = learned_fork(c, g, q, &lp);
+    return r ? r : enqueue_solve(c, g, d_inMST, &o, q, inner_events, &lp);
   };
   // A solve repeated with the same graph, buffers and options (benchmarks,
   // iterative callers) is captured once as a CUDA graph and then replayed
@@ -1424,9 +1473,16 @@ int batch_enqueue(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST, const 
                         b->eweight + b->edge_off[g]};
         ECL_CUDA_TRY(cudaMemsetAsync(c->big->st, 0, sizeof(DevState), q));
         mst_opts go = lo;
-        if (go.threshold_mode == ECL_THRESH_LEARNED && !(learned && dg.edges >= kLearnedMinEdges))
+        LearnedPlan lp{c->big->side, c->big->prep_done, c->big->join, nullptr};
+        const LearnedPlan* plan = nullptr;
+        if (learned && dg.edges >= kLearnedMinEdges) {
+          const int r = learned_fork(c->big, &dg, q, &lp);
+          if (r) return r;
+          plan = &lp;
+        } else if (go.threshold_mode == ECL_THRESH_LEARNED) {
           go.threshold_mode = ECL_THRESH_HEURISTIC;
-        int r = enqueue_solve(c->big, &dg, d_inMST + b->edge_off[g], &go, q, false);
+        }
+        int r = enqueue_solve(c->big, &dg, d_inMST + b->edge_off[g], &go, q, false, plan);
         if (r) return r;
         k_or_error<<<1, 1, 0, q>>>(c->big->st, c->st);
         ECL_CUDA_TRY(cudaGetLastError());

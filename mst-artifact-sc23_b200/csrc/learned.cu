@@ -3,13 +3,15 @@
 // inference, gradient and training (Adam) kernels. The network maps the
 // features to the light-phase filter quantile (output 0, as log2 q relative
 // to the reference heuristic's quantile) and the scan's degree split
-// (output 1, as log2 split). Only the schedule changes; the forest is unique
-// under the (weight, index) order, so the answer does not. The reference
-// heuristic (ECL_MST.cu:432-440) remains the fallback when no weights are
-// loaded. In a solve the network runs inside k_prep; the sample sort, the
-// features and the forward pass it uses are shared with this file's
-// standalone feature pass (learned_device.cuh, which also gives the
-// parameter blob layout).
+// (output 1, as log2 split). Only the schedule changes;
+// the forest is unique under the (weight, index) order, so the answer does
+// not (for non-negative weights). The reference heuristic (ECL_MST.cu:432-440)
+// remains the fallback when no weights are loaded.
+//
+// Parameter blob layout (kMlpParams floats):
+//   W1[16][64], b1[64], W2[64][64], b2[64], W3[64][2], b3[2], mean[16], std[16]
+// Features are standardised with mean/std before the first layer.
+#include <cub/block/block_radix_sort.cuh>
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -19,14 +21,19 @@
 
 #include "ecl_mst.h"
 #include "internal.h"
-#include "learned_device.cuh"
+#include "mst_kernels.cuh"
 
 namespace {
 
-using namespace ecl;
-constexpr int kIn = kMlpIn, kH = kMlpH, kOut = kMlpOut, kParams = kMlpParams, kTrainable = kMlpTrainable;
-constexpr int kSample = kFeatSample;
-constexpr int kMB = 64;  // training minibatch
+constexpr int kIn = ECL_MLP_INPUTS, kH = ECL_MLP_HIDDEN, kOut = ECL_MLP_OUTPUTS;
+constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kIn * kH, kOffW2 = kOffB1 + kH, kOffB2 = kOffW2 + kH * kH;
+constexpr int kOffW3 = kOffB2 + kH, kOffB3 = kOffW3 + kH * kOut, kOffMean = kOffB3 + kOut;
+constexpr int kOffStd = kOffMean + kIn, kParams = kOffStd + kIn;
+static_assert(kParams == ECL_MLP_PARAMS, "parameter blob size");
+constexpr int kTrainable = kOffMean;  // W1..b3
+constexpr int kMB = 64;               // training minibatch
+constexpr int kSample = 4096;         // weight sample for the quantile features
+constexpr float kNoFilterLog2Q = -0.32192809f;  // log2(0.8): predicted quantiles above run unfiltered
 
 int cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return ECL_OK;
@@ -41,17 +48,71 @@ int cuda_status(cudaError_t e) {
   } while (0)
 
 // ------------------------------------------------------------- features
-constexpr int kFeatThreads = 1024;
+using ecl::FeatAcc;
+using ecl::FeatPart;
 
-// The feature pass of a graph outside a solve (training sweeps): block 0
-// sorts the weight sample, the other blocks sum the degree statistics over
-// all vertices (grid-stride), as k_prep does inside a learned solve.
+constexpr int kFeatThreads = 1024;
+constexpr int kFeatKeys = kSample / kFeatThreads;
+
+#ifndef ECL_SAMPLE_BITONIC
+#define ECL_SAMPLE_BITONIC 0
+#endif
+
+// The 4096-entry hashed weight sample, sorted (a block radix sort, 4 keys per
+// thread) into `sorted`. One CTA of kFeatThreads.
+__device__ __forceinline__ void sort_sample(const int* eweight, int m, int* sorted) {
+#if ECL_SAMPLE_BITONIC
+  // bitonic network in shared memory: each thread takes two of the 2048
+  // compare-exchange pairs of every stage
+  __shared__ int a[kSample];
+  for (int i = threadIdx.x; i < kSample; i += blockDim.x) {
+    const uint64_t r = ecl_mix64(0xFEA70000ull + (uint64_t)i);
+    a[i] = m > 0 ? __ldg(eweight + (unsigned)(r % (uint64_t)(unsigned)m)) : 0;
+  }
+  __syncthreads();
+  for (int k = 2; k <= kSample; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int q = threadIdx.x; q < kSample / 2; q += blockDim.x) {
+        const int i = ((q & ~(j - 1)) << 1) | (q & (j - 1)), l = i + j;
+        const int x = a[i], y = a[l];
+        if ((x > y) == ((i & k) == 0)) {
+          a[i] = y;
+          a[l] = x;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < kSample; i += blockDim.x) sorted[i] = a[i];
+  return;
+#endif
+  typedef cub::BlockRadixSort<int, kFeatThreads, kFeatKeys> SampleSort;
+  __shared__ typename SampleSort::TempStorage sort_tmp;
+  int keys[kFeatKeys];
+#pragma unroll
+  for (int k = 0; k < kFeatKeys; k++) {
+    const int i = threadIdx.x * kFeatKeys + k;
+    const uint64_t r = ecl_mix64(0xFEA70000ull + (uint64_t)i);
+    keys[k] = m > 0 ? __ldg(eweight + (unsigned)(r % (uint64_t)(unsigned)m)) : 0;
+  }
+  SampleSort(sort_tmp).Sort(keys);  // blocked: thread t holds ranks t * kFeatKeys ...
+#pragma unroll
+  for (int k = 0; k < kFeatKeys; k++) sorted[threadIdx.x * kFeatKeys + k] = keys[k];
+}
+
+// The solve's share of the feature pass: the sorted weight sample (the
+// degree statistics come from k_prep).
+__global__ void __launch_bounds__(kFeatThreads) k_sample(const int* eweight, int m, int* sorted) {
+  sort_sample(eweight, m, sorted);
+}
+
+// The whole feature pass for a graph outside a solve: block 0 sorts the
+// weight sample, the other blocks take the degree statistics over all
+// vertices (grid-stride) exactly as k_prep does.
 __global__ void __launch_bounds__(kFeatThreads) k_feat(const int* nindex, int n, const int* eweight, int m,
                                                         FeatAcc* acc, int* sorted) {
   if (blockIdx.x == 0) {
-    __shared__ int samp[kSample];
-    sort_feat_sample(eweight, m, samp);
-    for (int i = threadIdx.x; i < kSample; i += blockDim.x) sorted[i] = samp[i];
+    sort_sample(eweight, m, sorted);
     return;
   }
   FeatPart fp;
@@ -68,12 +129,34 @@ int feat_grid(int nodes, int sms) {
   return 1 + std::max(1, std::min(sms * 2, (nodes + kFeatThreads - 1) / kFeatThreads));
 }
 
+// The 16 features (one thread), from the degree statistics and the sorted
+// weight sample.
+__device__ void compute_features(int n, int m, const FeatAcc* acc, const int* sorted, float* out) {
+  const double dn = (double)n, dm = (double)m;
+  const double mean = dm / dn;
+  const double var = fmax(0.0, (double)acc->deg_sq / dn - mean * mean);
+  const double wmax = fmax(1.0, (double)sorted[kSample - 1]);
+  const float qs[7] = {0.01f, 0.02f, 0.05f, 0.1f, 0.2f, 0.3f, 0.5f};
+  out[0] = (float)log2(dn);
+  out[1] = (float)log2(fmax(dm, 1.0));
+  out[2] = (float)log2(mean + 1.0);
+  out[3] = (float)log2((double)acc->max_deg + 1.0);
+  out[4] = (float)(sqrt(var) / fmax(mean, 1e-9));
+  out[5] = (float)((double)acc->zero / dn);
+  out[6] = (float)((double)acc->low / dn);
+  out[7] = (float)((double)acc->high / dn);
+  out[8] = (float)(3.0 * dn / fmax(dm, 1.0));  // the reference heuristic's "300% of nodes" quantile
+  for (int i = 0; i < 7; i++) out[9 + i] = (float)((double)sorted[(int)(qs[i] * (kSample - 1))] / wmax);
+}
+
 // The features alone (for training data): one thread.
 __global__ void k_feat_finish(int n, int m, const FeatAcc* acc, const int* sorted, float* out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) compute_features(n, m, *acc, sorted, out);
+  if (threadIdx.x == 0 && blockIdx.x == 0) compute_features(n, m, acc, sorted, out);
 }
 
 // ------------------------------------------------------------------- MLP
+__device__ __forceinline__ float relu(float x) { return x > 0.f ? x : 0.f; }
+
 // Forward pass of one sample held in x[kIn] (already standardised); h1, h2
 // and y are written. Serial per thread (the network is tiny).
 __device__ void mlp_forward1(const float* p, const float* x, float* h1, float* h2, float* y) {
@@ -101,6 +184,76 @@ __global__ void k_mlp_infer(const float* p, const float* x, int B, float* y) {
   float xs[kIn], h1[kH], h2[kH];
   for (int i = 0; i < kIn; i++) xs[i] = (x[b * kIn + i] - p[kOffMean + i]) / p[kOffStd + i];
   mlp_forward1(p, xs, h1, h2, y + b * kOut);
+}
+
+// log2 of the weight quantile the reference heuristic filters at
+// (ECL_MST.cu:408,432-440): the idx-th of 20 samples sits at quantile
+// (idx + 1) / 21 on average; 0 (no filter) when edges/nodes < 4.
+__host__ __device__ __forceinline__ float heuristic_log2_quantile(int n, int m) {
+  if (n < 1 || m / n < 4) return 0.f;
+  const int idx = min(19, (int)(3.0 * n * 20 / m));
+  return log2f((float)(idx + 1) / 21.f);
+}
+
+// Decode the network output into the solve's control block. Output 0 is the
+// log2 quantile relative to the reference heuristic's; output 1 the log2
+// degree split.
+// One CTA of kH threads: thread j computes hidden unit j of each layer. The
+// decoded quantile selects the light-phase threshold from the sorted weight
+// sample of the feature pass.
+__global__ void k_mlp_apply(const float* pg, const FeatAcc* acc, const int* sorted, int n, int m,
+                            ecl::DevState* st, float* feat_out) {
+  // the whole parameter blob (21 KB) is staged in shared memory first, so the
+  // layers read it at shared-memory latency instead of one global load per
+  // multiply-add
+  __shared__ float p[kParams];
+  __shared__ float fx[kIn], xs[kIn], h1[kH], h2[kH], y[kOut];
+  const int j = threadIdx.x;
+  for (int i = j; i < kParams; i += blockDim.x) p[i] = __ldg(pg + i);
+  if (j == 0) compute_features(n, m, acc, sorted, fx);
+  __syncthreads();
+  if (j < kIn) {
+    feat_out[j] = fx[j];  // kept for ecl_mst_ctx_learned_features
+    xs[j] = (fx[j] - p[kOffMean + j]) / p[kOffStd + j];
+  }
+  __syncthreads();
+  if (j < kH) {
+    float a = p[kOffB1 + j];
+    for (int i = 0; i < kIn; i++) a += xs[i] * p[kOffW1 + i * kH + j];
+    h1[j] = relu(a);
+  }
+  __syncthreads();
+  if (j < kH) {
+    float a = p[kOffB2 + j];
+    for (int i = 0; i < kH; i++) a += h1[i] * p[kOffW2 + i * kH + j];
+    h2[j] = relu(a);
+  }
+  __syncthreads();
+  if (j < kOut) {
+    float a = p[kOffB3 + j];
+    for (int i = 0; i < kH; i++) a += h2[i] * p[kOffW3 + i * kOut + j];
+    y[j] = a;
+  }
+  __syncthreads();
+  if (j != 0) return;
+  // output 0 (+ the heuristic's log2 quantile) at or above log2(0.8) means
+  // "no filter": a light phase holding 80 % of the entries or more is not
+  // worth a second phase (measured on the held-out sweeps)
+  const float lq = fminf(fmaxf(heuristic_log2_quantile(n, m) + y[0], -10.f), 0.f);
+  const float q = lq >= kNoFilterLog2Q ? 1.0f : exp2f(lq);
+  st->quantile = q;
+  if (q < 1.0f) {
+    int idx = (int)(q * (float)(kSample - 1));
+    idx = idx < 0 ? 0 : (idx > kSample - 1 ? kSample - 1 : idx);
+    st->filtered = 1;
+    st->threshold = sorted[idx];
+  } else {
+    st->filtered = 0;
+    st->threshold = 0x7fffffff;
+  }
+  // output 1: log2 of the degree split, in [1, 6]
+  st->learned_split = 1 << (int)lrintf(fminf(fmaxf(y[1], 1.f), 6.f));
+  st->split = st->learned_split;  // read by the scans (k_prep leaves it alone in this mode)
 }
 
 // Full-batch mean-squared-error loss and gradient of the trainable
@@ -202,7 +355,8 @@ unsigned g_w_version = 0;      // bumped by every load; contexts re-upload on ch
 }  // namespace
 
 struct ecl_mst_ctx;
-int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, unsigned** version);
+int ecl_ctx_learned_buffers(ecl_mst_ctx* c, float** params, float** feat, void** acc, int** sample,
+                            unsigned** version, int* sm_count);
 
 extern "C" int ecl_learned_set_weights(const float* params, int count) {
   if (count != kParams || !params) return ECL_ERR_INVALID_ARG;
@@ -230,9 +384,12 @@ unsigned ecl_learned_weights_version() {
 // changed since its last upload (synchronous: call it outside any stream
 // capture before capturing learned solves).
 int ecl_learned_upload(ecl_mst_ctx* c, cudaStream_t s) {
-  float* d_params;
+  float *d_params, *d_feat;
+  void* d_acc;
+  int* d_sample;
   unsigned* version;
-  int r = ecl_ctx_learned_buffers(c, &d_params, &version);
+  int sms = 0;
+  int r = ecl_ctx_learned_buffers(c, &d_params, &d_feat, &d_acc, &d_sample, &version, &sms);
   if (r) return r;
   std::lock_guard<std::mutex> lock(g_w_mu);
   if (g_weights.empty()) return ECL_ERR_UNSUPPORTED;
@@ -241,6 +398,39 @@ int ecl_learned_upload(ecl_mst_ctx* c, cudaStream_t s) {
     ML_TRY(cudaStreamSynchronize(s));
     *version = g_w_version;
   }
+  return ECL_OK;
+}
+
+// A learned solve's weight sample, sorted on stream s (after uploading the
+// loaded weights if they changed since this context's last upload).
+int ecl_learned_sample(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s) {
+  int r = ecl_learned_upload(c, s);
+  if (r) return r;
+  float *d_params, *d_feat;
+  void* d_acc;
+  int* d_sample;
+  unsigned* version;
+  int sms = 0;
+  if ((r = ecl_ctx_learned_buffers(c, &d_params, &d_feat, &d_acc, &d_sample, &version, &sms))) return r;
+  k_sample<<<1, kFeatThreads, 0, s>>>(g->eweight, g->edges, d_sample);
+  ML_TRY(cudaGetLastError());
+  return ECL_OK;
+}
+
+// The features (sorted sample + k_prep's degree statistics) and the MLP, on
+// stream s once both are complete; writes the decoded schedule into the
+// solve's control block `st`.
+int ecl_learned_apply(ecl_mst_ctx* c, const ecl_graph* g, cudaStream_t s, void* st) {
+  float *d_params, *d_feat;
+  void* d_acc;
+  int* d_sample;
+  unsigned* version;
+  int sms = 0;
+  int r = ecl_ctx_learned_buffers(c, &d_params, &d_feat, &d_acc, &d_sample, &version, &sms);
+  if (r) return r;
+  k_mlp_apply<<<1, 256, 0, s>>>(d_params, (const FeatAcc*)d_acc, d_sample, g->nodes, g->edges,
+                               (ecl::DevState*)st, d_feat);
+  ML_TRY(cudaGetLastError());
   return ECL_OK;
 }
 

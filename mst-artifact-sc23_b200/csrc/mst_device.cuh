@@ -32,7 +32,6 @@
 #include "ecl_mst.h"
 #include "internal.h"
 #include "mst_kernels.cuh"
-#include "learned_device.cuh"
 
 namespace ecl {
 
@@ -99,12 +98,7 @@ struct PrepArgs {
   int mode, explicit_thr, split;
   float quantile;
   DevState* st;
-  // learned schedule only (mode ECL_THRESH_LEARNED): the network's parameter
-  // blob on the device, and where the sorted weight sample and the features
-  // are kept
-  const float* mlp;
-  int* sample;
-  float* feat_out;
+  FeatAcc* feat;  // learned schedule: degree statistics gathered here, else null
 };
 
 struct ScanArgs {
@@ -172,19 +166,15 @@ constexpr unsigned kAblKeepEnds = kAblNoIPC | kAblNoTuples | kAblNoDD;
 // ------------------------------------------------------------------ prep
 // Threshold rule, by mode (run by one CTA). HEURISTIC restates main's rule
 // (ECL_MST.cu:408,432-440); QUANTILE takes a quantile of a 4096-entry hashed
-// sample; LEARNED sorts the network's weight sample into a.sample and leaves
-// the threshold, filter flag and split to the network, which the last CTA of
-// k_prep runs once the degree statistics are complete.
+// sample; LEARNED leaves the threshold, filter flag and split to the MLP
+// kernel (k_mlp_apply, which runs beside this kernel on another stream and
+// takes them from its own sorted sample).
 __device__ void choose_threshold(const PrepArgs& a, int* samp) {
   DevState* st = a.st;
   const int tid = threadIdx.x;
   int mode = a.mode, split = a.split;
   float quantile = a.quantile;
-  if (mode == ECL_THRESH_LEARNED) {
-    sort_feat_sample(a.eweight, a.edges, samp);
-    for (int i = tid; i < kFeatSample; i += blockDim.x) a.sample[i] = samp[i];
-    return;
-  }
+  if (mode == ECL_THRESH_LEARNED) return;
   const int nodes = a.nodes, edges = a.edges;
   if (tid == 0) st->split = split;
   if (mode == ECL_THRESH_NONE || (mode == ECL_THRESH_QUANTILE && !(quantile < 1.0f))) {
@@ -261,33 +251,9 @@ __device__ void choose_threshold(const PrepArgs& a, int* samp) {
   }
 }
 
-// The learned schedule's decision, by the CTA of k_prep that finishes last:
-// the features from the summed degree statistics and the sorted sample (both
-// complete: every CTA fenced its writes before counting itself done), then
-// the network.
-__device__ __noinline__ void learned_last_cta(const PrepArgs& a) {
-  __shared__ float fx[kMlpIn];
-  DevState* st = a.st;
-  __threadfence();
-  if (threadIdx.x == 0) {
-    FeatAcc acc;
-    acc.deg_sum = __ldcg(&st->feat.deg_sum);
-    acc.deg_sq = __ldcg(&st->feat.deg_sq);
-    acc.zero = __ldcg(&st->feat.zero);
-    acc.low = __ldcg(&st->feat.low);
-    acc.high = __ldcg(&st->feat.high);
-    acc.max_deg = __ldcg(&st->feat.max_deg);
-    compute_features(a.nodes, a.edges, acc, a.sample, fx);
-  }
-  __syncthreads();
-  mlp_decide(a.mlp, fx, a.sample, a.nodes, a.edges, st, a.feat_out);
-}
-
-__global__ void __launch_bounds__(kThreads, 4) k_prep(PrepArgs a) {
+__global__ void __launch_bounds__(kThreads) k_prep(PrepArgs a) {
   __shared__ int samp[4096];
-  __shared__ bool last;
   DevState* st = a.st;
-  const bool learned = a.mode == ECL_THRESH_LEARNED;
   if (blockIdx.x == 0) choose_threshold(a, samp);
   const int n = a.nodes, m = a.edges;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
@@ -300,7 +266,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_prep(PrepArgs a) {
     const int b = __ldg(a.nindex + v), e = __ldg(a.nindex + v + 1);
     const bool row_bad = b < 0 || e < b || e > m;
     bad |= row_bad;
-    if (learned) fp.add(e > b ? (unsigned)(e - b) : 0u);
+    if (a.feat) fp.add(e > b ? (unsigned)(e - b) : 0u);
     // Tile->vertex table (first_v[t] = row of entry t * kGran), first step:
     // the row holding the first step position at or after its start writes
     // itself there (each position has exactly one owner, so no conflicts);
@@ -311,13 +277,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_prep(PrepArgs a) {
   }
   if (gid == 0) bad |= __ldg(a.nindex) != 0 || __ldg(a.nindex + n) != m;
   if (bad) atomicOr(&st->error, kErrFormat);
-  if (!learned) return;  // uniform across the grid
-  fp.fold<kThreads>(&st->feat);
-  __threadfence();  // this thread's writes (the sums; block 0: the sorted sample) before the count
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(&st->feat_done, 1u) == gridDim.x - 1u;
-  __syncthreads();
-  if (last) learned_last_cta(a);
+  if (a.feat) fp.fold<kThreads>(a.feat);  // uniform across the grid
 }
 
 // Inclusive max scan of the tile->vertex table first_v[0 .. tiles), in

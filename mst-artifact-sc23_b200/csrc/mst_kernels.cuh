@@ -114,10 +114,6 @@ struct DevState {
   // barrier that ends the pass, read after it).
   unsigned seg_cnt[kMaxRoundCtas];
   unsigned seg_off[kMaxRoundCtas];
-  // learned schedule: the degree statistics k_prep sums, and the count of its
-  // CTAs done (the last one runs the network)
-  FeatAcc feat;
-  unsigned feat_done;
 };
 
 __device__ __forceinline__ u64 globaltimer_ns() {
