@@ -54,38 +54,9 @@ using ecl::FeatPart;
 constexpr int kFeatThreads = 1024;
 constexpr int kFeatKeys = kSample / kFeatThreads;
 
-#ifndef ECL_SAMPLE_BITONIC
-#define ECL_SAMPLE_BITONIC 0
-#endif
-
 // The 4096-entry hashed weight sample, sorted (a block radix sort, 4 keys per
 // thread) into `sorted`. One CTA of kFeatThreads.
 __device__ __forceinline__ void sort_sample(const int* eweight, int m, int* sorted) {
-#if ECL_SAMPLE_BITONIC
-  // bitonic network in shared memory: each thread takes two of the 2048
-  // compare-exchange pairs of every stage
-  __shared__ int a[kSample];
-  for (int i = threadIdx.x; i < kSample; i += blockDim.x) {
-    const uint64_t r = ecl_mix64(0xFEA70000ull + (uint64_t)i);
-    a[i] = m > 0 ? __ldg(eweight + (unsigned)(r % (uint64_t)(unsigned)m)) : 0;
-  }
-  __syncthreads();
-  for (int k = 2; k <= kSample; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int q = threadIdx.x; q < kSample / 2; q += blockDim.x) {
-        const int i = ((q & ~(j - 1)) << 1) | (q & (j - 1)), l = i + j;
-        const int x = a[i], y = a[l];
-        if ((x > y) == ((i & k) == 0)) {
-          a[i] = y;
-          a[l] = x;
-        }
-      }
-      __syncthreads();
-    }
-  }
-  for (int i = threadIdx.x; i < kSample; i += blockDim.x) sorted[i] = a[i];
-  return;
-#endif
   typedef cub::BlockRadixSort<int, kFeatThreads, kFeatKeys> SampleSort;
   __shared__ typename SampleSort::TempStorage sort_tmp;
   int keys[kFeatKeys];

@@ -72,9 +72,6 @@ constexpr int kSplitAfter = 8;         // find steps before path splitting start
 #ifndef ECL_FLAT_ROUNDS
 #define ECL_FLAT_ROUNDS 2
 #endif
-#ifndef ECL_FLAT_CACHE
-#define ECL_FLAT_CACHE 0
-#endif
 #ifndef ECL_L2_HINTS
 #define ECL_L2_HINTS 1                 // evict-first CSR streams, evict-last parent gathers in the scans
 #endif
@@ -1397,16 +1394,7 @@ __global__ void __launch_bounds__(kRoundThreads, ECL_ROUND_MIN_BLOCKS) k_rounds(
                       (unsigned long long)W >= (unsigned long long)ECL_FLAT_ROUNDS * (unsigned)a.nodes;
     if (flat) {
       for (int v = (int)(start * blockDim.x + threadIdx.x); v < a.nodes; v += (int)(stride * blockDim.x)) {
-#if ECL_FLAT_CACHE
-        // walks through the CTA's find cache: the nodes near the top of a
-        // large tree, which every walk in it reaches, are read once per CTA
-        int x[1] = {v};
-        const bool ok[1] = {true};
-        multi_find<1>(x, ok, a.parent, s);
-        const int rt = x[0];
-#else
         const int rt = find_ro(v, a.parent);
-#endif
         if (rt != v) __stcg(a.parent + v, rt);
       }
       if (!grid_barrier(st, kBarrierTimeoutNs, active)) return;
