@@ -256,7 +256,13 @@ typedef struct mst_opts {
                           /* CSR entries (and fitting the per-CTA scratch) are */
                           /* solved one per CTA by the persistent kernel;      */
                           /* 0 = the context's per-CTA capacity                */
-  int32_t reserved[7];
+  int32_t batch_large_streams; /* batched mode: the other graphs are solved on */
+                          /* this many concurrent streams (1..8), each with    */
+                          /* its own workspace, largest graph first to the     */
+                          /* least-loaded stream; with more than one, their    */
+                          /* round kernels take one CTA per SM unless          */
+                          /* ctas_per_sm is set; 0 = default (4)               */
+  int32_t reserved[6];
 } mst_opts;
 
 /* Fill *opts with the defaults (heuristic threshold, reference semantics). */
@@ -418,9 +424,10 @@ int ecl_mst_run_batch_device(ecl_batch_ctx* ctx, const ecl_batch* batch,
 
 /* Autotuner: times candidate schedules (per-CTA cutoff, scan entries per
  * thread and, when *base asks for the learned schedule, learned against the
- * reference heuristic for the large graphs) on the batch and writes the
- * fastest into *best (a copy of *base with those fields set). The answer is
- * the same for every candidate; only the time differs. */
+ * reference heuristic for the large graphs; then, unless *base sets them,
+ * the large graphs' streams and round-kernel CTAs per SM) on the batch and
+ * writes the fastest into *best (a copy of *base with those fields set).
+ * The answer is the same for every candidate; only the time differs. */
 int ecl_batch_autotune(ecl_batch_ctx* ctx, const ecl_batch* batch, uint8_t* d_inMST,
                        const mst_opts* base, mst_opts* best, float* best_ms);
 
