@@ -253,7 +253,8 @@ def batch_leg(args, E, torch, dev, rank=0, world=1, dist=None, mode=None):
            "graphs_large": last["graphs_large"], "cuda_graph_replay": last["graph_replay"],
            "ms_small": last["ms_small"], "ms_large": last["ms_large"],
            "autotuned": {"batch_small_edges": best.batch_small_edges, "degree_split": best.degree_split,
-                         "small_tail": best.small_tail},
+                         "small_tail": best.small_tail, "batch_large_streams": best.batch_large_streams,
+                         "ctas_per_sm": best.ctas_per_sm},
            "schedule": {E.THRESH_LEARNED: "learned (large graphs) / heuristic (per-CTA graphs)"}.get(
                best.threshold_mode, "heuristic"),
            "generated_on": "device" if on_device else "host", "gen_s": round(gen_s, 1),
