@@ -254,7 +254,7 @@ def batch_leg(args, E, torch, dev, rank=0, world=1, dist=None, mode=None):
            "ms_small": last["ms_small"], "ms_large": last["ms_large"],
            "autotuned": {"batch_small_edges": best.batch_small_edges, "degree_split": best.degree_split,
                          "small_tail": best.small_tail, "batch_large_streams": best.batch_large_streams,
-                         "ctas_per_sm": best.ctas_per_sm, "batch_small_ctas_per_sm": best.batch_small_ctas_per_sm},
+                         "ctas_per_sm": best.ctas_per_sm},
            "schedule": {E.THRESH_LEARNED: "learned (large graphs) / heuristic (per-CTA graphs)"}.get(
                best.threshold_mode, "heuristic"),
            "generated_on": "device" if on_device else "host", "gen_s": round(gen_s, 1),

@@ -262,11 +262,7 @@ typedef struct mst_opts {
                           /* least-loaded stream; with more than one, their    */
                           /* round kernels take one CTA per SM unless          */
                           /* ctas_per_sm is set; 0 = default (4)               */
-  int32_t batch_small_ctas_per_sm; /* batched mode: > 0 runs the one-graph-per- */
-                          /* CTA kernel with this many CTAs per SM on its own  */
-                          /* stream, beside the large graphs; 0 = every        */
-                          /* resident CTA slot, before the large graphs        */
-  int32_t reserved[5];
+  int32_t reserved[6];
 } mst_opts;
 
 /* Fill *opts with the defaults (heuristic threshold, reference semantics). */
@@ -429,8 +425,7 @@ int ecl_mst_run_batch_device(ecl_batch_ctx* ctx, const ecl_batch* batch,
 /* Autotuner: times candidate schedules (per-CTA cutoff, scan entries per
  * thread and, when *base asks for the learned schedule, learned against the
  * reference heuristic for the large graphs; then, unless *base sets them,
- * the large graphs' streams and round-kernel CTAs per SM, and the per-CTA
- * kernel beside the large graphs at 1 or 2 CTAs per SM) on the batch and
+ * the large graphs' streams and round-kernel CTAs per SM) on the batch and
  * writes the fastest into *best (a copy of *base with those fields set).
  * The answer is the same for every candidate; only the time differs. */
 int ecl_batch_autotune(ecl_batch_ctx* ctx, const ecl_batch* batch, uint8_t* d_inMST,

@@ -749,7 +749,6 @@ int check_opts(const mst_opts* o) {
   if (o->degree_split < 0 || o->degree_split > (1 << 20)) return ECL_ERR_INVALID_ARG;
   if (o->ctas_per_sm < 0) return ECL_ERR_INVALID_ARG;
   if (o->batch_large_streams < 0 || o->batch_large_streams > 8) return ECL_ERR_INVALID_ARG;
-  if (o->batch_small_ctas_per_sm < 0) return ECL_ERR_INVALID_ARG;
   if (o->threshold_mode == ECL_THRESH_QUANTILE && !(o->quantile >= 0.0f)) return ECL_ERR_INVALID_ARG;
   return ECL_OK;
 }
@@ -1291,11 +1290,7 @@ struct ecl_batch_ctx {
   // more streams (opts batch_large_streams)
   ecl_mst_ctx* big[kMaxLargeStreams] = {};
   cudaEvent_t large_fork = nullptr, large_join[kMaxLargeStreams] = {};
-  // the per-CTA kernel's stream when it runs beside the large graphs
-  cudaStream_t small_stream = nullptr;
-  cudaEvent_t small_fork = nullptr, small_done = nullptr;
-  cudaEvent_t ev[4] = {};  // start, small graphs done, all done, large graphs done
-  bool overlapped = false;  // the last batch ran its two parts side by side
+  cudaEvent_t ev[3] = {};
   // the large-graph launch sequence captured as a CUDA graph, keyed by the batch
   cudaGraphExec_t exec = nullptr;
   std::vector<long long> exec_key;
@@ -1330,10 +1325,6 @@ extern "C" void ecl_batch_ctx_destroy(ecl_batch_ctx* c) {
   cudaFree(c->st);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
-  if (c->small_stream) cudaStreamSynchronize(c->small_stream);
-  if (c->small_fork) cudaEventDestroy(c->small_fork);
-  if (c->small_done) cudaEventDestroy(c->small_done);
-  if (c->small_stream) cudaStreamDestroy(c->small_stream);
   if (c->large_fork) cudaEventDestroy(c->large_fork);
   for (auto& e : c->large_join)
     if (e) cudaEventDestroy(e);
@@ -1383,9 +1374,6 @@ extern "C" int ecl_batch_ctx_create(int device, int32_t max_graphs, int64_t max_
   for (auto& e : c->ev)
     if ((st = cuda_status(cudaEventCreate(&e)))) return fail(st);
   if ((st = cuda_status(cudaEventCreateWithFlags(&c->large_fork, cudaEventDisableTiming)))) return fail(st);
-  if ((st = cuda_status(cudaStreamCreateWithFlags(&c->small_stream, cudaStreamNonBlocking)))) return fail(st);
-  if ((st = cuda_status(cudaEventCreateWithFlags(&c->small_fork, cudaEventDisableTiming)))) return fail(st);
-  if ((st = cuda_status(cudaEventCreateWithFlags(&c->small_done, cudaEventDisableTiming)))) return fail(st);
   for (auto& e : c->large_join)
     if ((st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)))) return fail(st);
   if (max_graph_edges > c->cap || max_graph_nodes > c->cap)
@@ -1432,21 +1420,12 @@ int batch_enqueue(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST, const 
   ECL_CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevState), s));
   ECL_CUDA_TRY(cudaMemsetAsync(c->d_queue, 0, sizeof(unsigned), s));
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  // With batch_small_ctas_per_sm set, the per-CTA kernel takes that many CTAs
-  // per SM on its own stream and runs beside the large graphs; otherwise it
-  // takes every resident CTA slot and runs first.
-  const bool overlap = o->batch_small_ctas_per_sm > 0 && S > 0 && !large.empty();
-  const cudaStream_t ss = overlap ? c->small_stream : s;
-  if (overlap) {
-    ECL_CUDA_TRY(cudaEventRecord(c->small_fork, s));
-    ECL_CUDA_TRY(cudaStreamWaitEvent(ss, c->small_fork, 0));
-  }
   if (S > 0) {
     ECL_CUDA_TRY(cudaMemcpyAsync(c->d_node_off, noff.data(), noff.size() * sizeof(long long),
-                                 cudaMemcpyHostToDevice, ss));
+                                 cudaMemcpyHostToDevice, s));
     ECL_CUDA_TRY(cudaMemcpyAsync(c->d_edge_off, eoff.data(), eoff.size() * sizeof(long long),
-                                 cudaMemcpyHostToDevice, ss));
-    ECL_CUDA_TRY(cudaMemcpyAsync(c->d_small, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice, ss));
+                                 cudaMemcpyHostToDevice, s));
+    ECL_CUDA_TRY(cudaMemcpyAsync(c->d_small, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice, s));
     BatchArgs ba;
     ba.num_small = S;
     ba.small_list = c->d_small;
@@ -1468,13 +1447,11 @@ int batch_enqueue(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST, const 
     ba.quantile = o->quantile;
     ba.count_atomics = (o->flags & ECL_FLAG_STATS) ? 1 : 0;
     ba.abl = round_ablation(o->flags);
-    const int grid = std::min(overlap ? std::min(c->small_grid, o->batch_small_ctas_per_sm * c->sm_count)
-                                      : c->small_grid, S);
-    k_batch_small<<<grid, kThreads, 0, ss>>>(ba);
+    const int grid = std::min(c->small_grid, S);
+    k_batch_small<<<grid, kThreads, 0, s>>>(ba);
     ECL_CUDA_TRY(cudaGetLastError());
   }
-  if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[1], ss));
-  if (overlap) ECL_CUDA_TRY(cudaEventRecord(c->small_done, ss));
+  if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   bool replayed = false;
   if (!large.empty()) {
     // The large graphs' launch sequence (per graph: control-block reset and
@@ -1598,10 +1575,7 @@ int batch_enqueue(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST, const 
       }
     }
   }
-  if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[3], s));
-  if (overlap) ECL_CUDA_TRY(cudaStreamWaitEvent(s, c->small_done, 0));
   if (timed) ECL_CUDA_TRY(cudaEventRecord(c->ev[2], s));
-  c->overlapped = overlap;
   if (stats) {
     memset(stats, 0, sizeof(*stats));
     stats->graphs_small = S;
@@ -1619,9 +1593,7 @@ int batch_finish(ecl_batch_ctx* c, cudaStream_t s, ecl_batch_stats* stats) {
   if (stats) {
     stats->status = (int32_t)err;
     cudaEventElapsedTime(&stats->ms_small, c->ev[0], c->ev[1]);
-    // beside each other both parts start at ev[0]; in sequence the large
-    // graphs start when the small ones are done
-    cudaEventElapsedTime(&stats->ms_large, c->overlapped ? c->ev[0] : c->ev[1], c->ev[3]);
+    cudaEventElapsedTime(&stats->ms_large, c->ev[1], c->ev[2]);
     cudaEventElapsedTime(&stats->ms_total, c->ev[0], c->ev[2]);
   }
   return device_error_status(err);
@@ -1704,25 +1676,6 @@ extern "C" int ecl_batch_autotune(ecl_batch_ctx* c, const ecl_batch* b, uint8_t*
           best_o = o;
         }
       }
-  }
-  // then the per-CTA kernel beside the large graphs
-  if (best_o.batch_small_ctas_per_sm == 0) {
-    const mst_opts o2 = best_o;
-    for (int scps : {1, 2}) {
-      mst_opts o = o2;
-      o.batch_small_ctas_per_sm = scps;
-      float t = 0.f;
-      for (int rep = 0; rep < 2; rep++) {
-        ecl_batch_stats bs;
-        int st = ecl_mst_run_batch_device(c, b, d_inMST, &o, nullptr, &bs);
-        if (st) return st;
-        if (rep > 0) t += bs.ms_total;
-      }
-      if (t < best_t) {
-        best_t = t;
-        best_o = o;
-      }
-    }
   }
   *best = best_o;
   if (best_ms) *best_ms = best_t;

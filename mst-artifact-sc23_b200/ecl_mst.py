@@ -53,8 +53,7 @@ class MstOpts(ctypes.Structure):
     _fields_ = [("threshold_mode", c_int32), ("threshold", c_int32), ("quantile", c_float),
                 ("degree_split", c_int32), ("round_min_tiles", c_int32), ("ctas_per_sm", c_int32),
                 ("small_tail", c_int32), ("flags", c_int32), ("batch_small_edges", c_int32),
-                ("batch_large_streams", c_int32), ("batch_small_ctas_per_sm", c_int32),
-                ("reserved", c_int32 * 5)]
+                ("batch_large_streams", c_int32), ("reserved", c_int32 * 6)]
 
 
 class MstStats(ctypes.Structure):
@@ -436,7 +435,7 @@ def heuristic_threshold(g):
 
 
 def make_opts(mode=THRESH_HEURISTIC, threshold=0, quantile=1.0, degree_split=0, small_tail=0, flags=0,
-              round_min_tiles=0, ctas_per_sm=0, batch_large_streams=0, batch_small_ctas_per_sm=0):
+              round_min_tiles=0, ctas_per_sm=0, batch_large_streams=0):
     o = MstOpts()
     load().ecl_default_opts(ctypes.byref(o))
     o.threshold_mode = mode
@@ -448,7 +447,6 @@ def make_opts(mode=THRESH_HEURISTIC, threshold=0, quantile=1.0, degree_split=0, 
     o.round_min_tiles = round_min_tiles
     o.ctas_per_sm = ctas_per_sm
     o.batch_large_streams = batch_large_streams
-    o.batch_small_ctas_per_sm = batch_small_ctas_per_sm
     return o
 
 

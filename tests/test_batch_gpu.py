@@ -69,15 +69,14 @@ def test_batch_mixed_small_and_large():
     assert sts[1]["graph_replay"] == 1
 
 
-@pytest.mark.parametrize("streams,cps,small_cps", [(1, 0, 0), (3, 0, 1), (8, 2, 0), (0, 0, 2)])
-def test_batch_large_graphs_on_concurrent_streams(streams, cps, small_cps):
+@pytest.mark.parametrize("streams,cps", [(1, 0), (3, 0), (8, 2), (0, 0)])
+def test_batch_large_graphs_on_concurrent_streams(streams, cps):
     """The graphs beyond the per-CTA cutoff spread over 1, 3 or 8 concurrent
     streams (each with its own engine; largest first to the least-loaded
-    stream) or the default, with the per-CTA kernel before them or beside
-    them; every graph keeps the oracle's forest, directly and from the
-    replayed capture."""
-    kw = dict(batch_large_streams=streams, ctas_per_sm=cps, batch_small_ctas_per_sm=small_cps)
-    opts = [E.make_opts(**kw), E.make_opts(mode=E.THRESH_QUANTILE, quantile=0.1, **kw)]
+    stream) or the default; every graph keeps the oracle's forest, directly
+    and from the replayed capture."""
+    opts = [E.make_opts(batch_large_streams=streams, ctas_per_sm=cps),
+            E.make_opts(mode=E.THRESH_QUANTILE, quantile=0.1, batch_large_streams=streams, ctas_per_sm=cps)]
     sts = _run(_mixed_graphs(5000, 40), 1 << 11, opts)
     assert all(s["graphs_large"] >= 8 and s["status"] == 0 for s in sts)
     assert sts[1]["graph_replay"] == 1 and sts[3]["graph_replay"] == 1
