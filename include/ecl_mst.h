@@ -261,7 +261,8 @@ typedef struct mst_opts {
                           /* its own workspace, largest graph first to the     */
                           /* least-loaded stream; with more than one, their    */
                           /* round kernels take one CTA per SM unless          */
-                          /* ctas_per_sm is set; 0 = default (4)               */
+                          /* ctas_per_sm is set; 0 = default (4); fewer when   */
+                          /* the device has no room for another workspace      */
   int32_t reserved[6];
 } mst_opts;
 

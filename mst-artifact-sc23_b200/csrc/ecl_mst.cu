@@ -1490,15 +1490,21 @@ int batch_enqueue(ecl_batch_ctx* c, const ecl_batch* b, uint8_t* d_inMST, const 
     // first, each to the stream with the fewest entries so far. With several
     // streams the round kernels take one CTA per SM unless ctas_per_sm says
     // otherwise, so the streams' rounds run side by side.
-    const int K = std::max(1, std::min((int)large.size(), o->batch_large_streams > 0
-                                                             ? std::min(o->batch_large_streams, kMaxLargeStreams)
-                                                             : kDefaultLargeStreams));
-    if (K > 1 && lo.ctas_per_sm == 0) lo.ctas_per_sm = 1;
+    int K = std::max(1, std::min((int)large.size(), o->batch_large_streams > 0
+                                                       ? std::min(o->batch_large_streams, kMaxLargeStreams)
+                                                       : kDefaultLargeStreams));
     for (int k = 0; k < K; k++) {
       int r = batch_big_ctx(c, k);
+      if (r == ECL_ERR_ALLOC && k > 0) {  // no room for another engine: fewer streams
+        cudaGetLastError();
+        K = k;
+        break;
+      }
       if (!r && learned) r = ecl_learned_upload(c->big[k], s);  // before any capture
       if (r) return r;
     }
+    if (K > 1 && lo.ctas_per_sm == 0) lo.ctas_per_sm = 1;
+    key.push_back(K);  // the streams in use (fewer than asked when memory ran short)
     std::vector<int> order(large);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->edges[x] > b->edges[y]; });
     std::vector<int> lane_of(order.size());
