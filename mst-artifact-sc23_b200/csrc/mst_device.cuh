@@ -362,7 +362,10 @@ enum ScanKind { kLight = 0, kHeavy = 1 };
 // entries (x = -1), which the first round skips.
 constexpr int kScanWarps = 8;                        // consumer warps of a scan CTA
 constexpr int kScanThreads = (kScanWarps + 1) * 32;  // plus the producer warp
-constexpr int kScanSegCap = 2048;                    // longest nindex slice (vertices) staged per tile
+#ifndef ECL_SCAN_SEGCAP
+#define ECL_SCAN_SEGCAP 2048
+#endif
+constexpr int kScanSegCap = ECL_SCAN_SEGCAP;         // longest nindex slice (vertices) staged per tile
 constexpr unsigned kScanMaxChunk = 64;               // worklist slots a warp reserves at once
 
 // ring stages and the resident CTAs per SM the launch bounds ask for, per EPT
