@@ -426,7 +426,8 @@ int ecl_mst_run_batch_device(ecl_batch_ctx* ctx, const ecl_batch* batch,
 /* Autotuner: times candidate schedules (per-CTA cutoff, scan entries per
  * thread and, when *base asks for the learned schedule, learned against the
  * reference heuristic for the large graphs; then, unless *base sets them,
- * the large graphs' streams and round-kernel CTAs per SM) on the batch and
+ * the large graphs' streams and round-kernel CTAs per SM, and the cutoff
+ * again with those) on the batch and
  * writes the fastest into *best (a copy of *base with those fields set).
  * The answer is the same for every candidate; only the time differs. */
 int ecl_batch_autotune(ecl_batch_ctx* ctx, const ecl_batch* batch, uint8_t* d_inMST,

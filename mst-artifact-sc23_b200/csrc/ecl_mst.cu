@@ -1634,35 +1634,40 @@ extern "C" int ecl_batch_autotune(ecl_batch_ctx* c, const ecl_batch* b, uint8_t*
   else ecl_default_opts(&o0);
   float best_t = 1e30f;
   mst_opts best_o = o0;
+  // one candidate: a warm-up run (which also captures), then a timed one
+  auto trial = [&](const mst_opts& o) -> int {
+    float t = 0.f;
+    for (int rep = 0; rep < 2; rep++) {
+      ecl_batch_stats bs;
+      const int st = ecl_mst_run_batch_device(c, b, d_inMST, &o, nullptr, &bs);
+      if (st) return st;
+      if (rep > 0) t += bs.ms_total;
+    }
+    if (t < best_t) {
+      best_t = t;
+      best_o = o;
+    }
+    return ECL_OK;
+  };
+  int st;
   const int cutoffs[] = {c->cap / 8, c->cap / 4, c->cap / 2, c->cap};
-  const int splits[] = {8, 16};
-  // The learned schedule (large graphs only) is kept only where it beats the
-  // reference heuristic on this batch.
+  // 1. per-CTA cutoff, scan entries per lane and schedule. The learned
+  //    schedule (large graphs only) is kept only where it beats the
+  //    reference heuristic on this batch.
   const int modes[] = {o0.threshold_mode, ECL_THRESH_HEURISTIC};
   const int nmodes = o0.threshold_mode == ECL_THRESH_LEARNED ? 2 : 1;
-  for (int mi = 0; mi < nmodes; mi++) {
+  for (int mi = 0; mi < nmodes; mi++)
     for (int cut : cutoffs) {
       if (cut < 1) continue;
-      for (int sp : splits) {
+      for (int sp : {8, 16}) {
         mst_opts o = o0;
         o.threshold_mode = modes[mi];
         o.batch_small_edges = cut;
         o.degree_split = sp;
-        float t = 0.f;
-        for (int rep = 0; rep < 2; rep++) {
-          ecl_batch_stats bs;
-          int st = ecl_mst_run_batch_device(c, b, d_inMST, &o, nullptr, &bs);
-          if (st) return st;
-          if (rep > 0) t += bs.ms_total;  // the first run warms up (and captures)
-        }
-        if (t < best_t) {
-          best_t = t;
-          best_o = o;
-        }
+        if ((st = trial(o))) return st;
       }
     }
-  }
-  // then the large graphs' concurrency around the best of those
+  // 2. the large graphs' streams and round CTAs per SM, unless *base sets them
   if (best_o.batch_large_streams == 0 && best_o.ctas_per_sm == 0) {
     const mst_opts o1 = best_o;
     for (int k : {1, 2, 4, 8})
@@ -1670,18 +1675,16 @@ extern "C" int ecl_batch_autotune(ecl_batch_ctx* c, const ecl_batch* b, uint8_t*
         mst_opts o = o1;
         o.batch_large_streams = k;
         o.ctas_per_sm = cps;
-        float t = 0.f;
-        for (int rep = 0; rep < 2; rep++) {
-          ecl_batch_stats bs;
-          int st = ecl_mst_run_batch_device(c, b, d_inMST, &o, nullptr, &bs);
-          if (st) return st;
-          if (rep > 0) t += bs.ms_total;
-        }
-        if (t < best_t) {
-          best_t = t;
-          best_o = o;
-        }
+        if ((st = trial(o))) return st;
       }
+    // 3. the cutoff again, now that the large graphs run concurrently
+    const mst_opts o2 = best_o;
+    for (int cut : cutoffs) {
+      if (cut < 1 || cut == o2.batch_small_edges) continue;
+      mst_opts o = o2;
+      o.batch_small_edges = cut;
+      if ((st = trial(o))) return st;
+    }
   }
   *best = best_o;
   if (best_ms) *best_ms = best_t;
