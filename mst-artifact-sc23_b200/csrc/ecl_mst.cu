@@ -486,6 +486,7 @@ int launch_scan(int ept, const ScanArgs& sa, cudaStream_t s, const cudaAccessPol
 template <int KIND>
 int launch_scans(ecl_mst_ctx* c, bool device_split, int split, const ScanArgs& sa, cudaStream_t s,
                  const cudaAccessPolicyWindow* win) {
+  if (KIND == kHeavy && ECL_HEAVY_EPT) return launch_scan<KIND>(ECL_HEAVY_EPT, sa, s, win);
   if (!device_split) return launch_scan<KIND>(scan_ept(split), sa, s, win);
   const cudaStream_t br[2] = {c->side, c->side2};
   ECL_CUDA_TRY(cudaEventRecord(c->scan_fork, s));
@@ -1245,7 +1246,7 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   const int fgrid = (int)std::min<int64_t>(((int64_t)n + kThreads - 1) / kThreads, (int64_t)d->sm_count * 16);
   k_flatten<<<std::max(fgrid, 1), kThreads, 0, s>>>(parent, n, dst);
   ECL_CUDA_TRY(cudaGetLastError());
-  if ((st = launch_scan<kHeavy>(scan_ept(split), sa, s))) return st;
+  if ((st = launch_scan<kHeavy>(heavy_ept(split), sa, s))) return st;
   ra.phase = 1;
   if ((st = launch_coop((const void*)k_rounds, rgrid, kRoundThreads, &ra, s))) return st;
   // Report device-side errors (malformed CSR, worklist overflow) to the caller.
