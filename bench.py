@@ -790,9 +790,9 @@ def main():
                     "sync": {"value": world * g.edges / e2e_sync / 1e9, "ms": e2e_sync * 1e3,
                              "what": "one blocking ecl_mst_ctx_run_host call per step"}},
             # per solve: k_prep, k_fill_chunks, k_fill_carry, k_scan x2, k_rounds x2, k_flatten; the
-            # learned schedule adds k_feat_degrees, k_feat_finish, k_mlp_apply and launches all
-            # three scan variants per phase (the two not selected exit at once)
-            "gpu_launches": (15 if args.mode == "learned" else 8) * args.steps,
+            # learned schedule adds k_sample and k_mlp_apply and launches all three light-scan
+            # variants (the two its split does not select exit at once; the heavy scan is one)
+            "gpu_launches": (12 if args.mode == "learned" else 8) * args.steps,
             "ablation": ablation,
             "heuristic_schedule": ({"value": world * g.edges / (np.mean(heur_ms) * 1e-3) / 1e9,
                                     "ms": float(np.mean(heur_ms)),
