@@ -238,11 +238,12 @@ typedef struct mst_opts {
   int32_t threshold;      /* ECL_THRESH_EXPLICIT: edges with w <= threshold    */
                           /* form the first (light) phase                      */
   float quantile;         /* ECL_THRESH_QUANTILE, in [0,1]; >= 1 disables      */
-  int32_t degree_split;   /* thread/cooperative split of the CSR scans: each   */
-                          /* thread takes E consecutive entries, E = 4 for     */
-                          /* split <= 4, 8 for split <= 8, else 16; rows       */
+  int32_t degree_split;   /* thread/cooperative split of the light CSR scan:   */
+                          /* each thread takes E consecutive entries, E = 4    */
+                          /* for split <= 4, 8 for split <= 8, else 16; rows   */
                           /* shorter than E stay in one thread, longer rows    */
-                          /* are spread over threads/warps; 0 = default (8)    */
+                          /* are spread over threads/warps; 0 = default (8).   */
+                          /* The heavy scan always takes E = 4                 */
   int32_t round_min_tiles; /* the round kernel keeps one CTA per this many   */
                           /* 512-entry tiles of a round's worklist: CTAs       */
                           /* beyond it leave the launch as the rounds shrink,  */
@@ -274,7 +275,7 @@ void ecl_default_opts(mst_opts* opts);
 typedef struct ecl_mst_stats {
   int32_t threshold;       /* threshold used (INT32_MAX when unfiltered)        */
   int32_t filtered;        /* 1 if two phases ran                               */
-  int32_t degree_split;    /* split used by the scans                           */
+  int32_t degree_split;    /* split used by the light scan                      */
   int32_t rounds[2];       /* Boruvka rounds of the light / heavy phase         */
   int32_t status;          /* device error word (0 = clean)                     */
   int64_t scan_kept[2];    /* worklist entries appended by each scan            */
