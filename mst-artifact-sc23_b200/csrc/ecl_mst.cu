@@ -821,12 +821,12 @@ int run_device_once(ecl_mst_ctx* c, const ecl_graph* g, uint8_t* d_inMST, const 
   // replay is timed as a whole (events around the launch), so its stats have
   // ms_total but no per-phase breakdown; ECL_FLAG_NO_GRAPH keeps the direct
   // launches and the breakdown.
-  float qbits;
+  int32_t qbits;  // the quantile's bit pattern
   memcpy(&qbits, &o.quantile, sizeof(qbits));
   const std::vector<long long> key = {
       g->nodes, g->edges, (long long)(uintptr_t)g->nindex, (long long)(uintptr_t)g->nlist,
       (long long)(uintptr_t)g->eweight, (long long)(uintptr_t)d_inMST, o.threshold_mode, o.threshold,
-      (long long)*(const int*)&qbits, o.degree_split, o.small_tail, o.flags, o.round_min_tiles, o.ctas_per_sm,
+      (long long)qbits, o.degree_split, o.small_tail, o.flags, o.round_min_tiles, o.ctas_per_sm,
       (long long)(uintptr_t)c->wl[0], (long long)ecl_learned_weights_version()};
   const bool graph_ok = !(o.flags & ECL_FLAG_NO_GRAPH);
   bool replayed = false;
@@ -1206,7 +1206,8 @@ extern "C" int ecl_mst_run_device_noalloc(const ecl_graph* g, uint8_t* d_inMST,
   pa.split = split;
   pa.quantile = o.quantile;
   pa.st = dst;
-  if ((st = enqueue_prep(pa, d->sm_count, s))) return st;
+  st = enqueue_prep(pa, d->sm_count, s);
+  if (st) return st;
   ScanArgs sa{};
   sa.nodes = n;
   sa.edges = m;
