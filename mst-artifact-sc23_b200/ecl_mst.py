@@ -415,6 +415,10 @@ class DeviceBatch:
         _check(self._lib.ecl_graph_to_host(ctypes.byref(gc), ctypes.byref(h)), "graph_to_host")
         return Graph._from_c(h)
 
+    def select(self, idx):
+        """A view of graphs `idx` of this batch (see ``BatchView``)."""
+        return BatchView(self, idx)
+
     def close(self):
         if self.c.nindex:
             self._lib.ecl_free_device_batch(ctypes.byref(self.c))
@@ -604,6 +608,41 @@ class Batch:
     def slice(self, inmst, g):
         a = int(self.edge_off[g])
         return inmst[a:a + int(self.edges[g])]
+
+    def select(self, idx):
+        """A view of graphs `idx` of this batch (see ``BatchView``)."""
+        return BatchView(self, idx)
+
+
+class BatchView:
+    """Graphs `idx` of a packed batch (``Batch`` or ``DeviceBatch``), in that
+    order, without copying their entries: the per-graph tables are subsets of
+    the parent's, so the view's graphs read the parent's packed arrays and
+    write their inMST at the parent's offsets of a full-size output buffer
+    (``total_edges`` is the parent's). This is how a rank solves its shard of
+    a batch (shard.partition_by_cost)."""
+
+    def __init__(self, parent, idx):
+        self.parent = parent
+        self.idx = np.asarray(idx, np.int64)
+        self.num_graphs = len(self.idx)
+        self.nodes = np.ascontiguousarray(parent.nodes[self.idx], np.int32)
+        self.edges = np.ascontiguousarray(parent.edges[self.idx], np.int32)
+        self.nindex_off = np.ascontiguousarray(parent.nindex_off[self.idx], np.int64)
+        self.edge_off = np.ascontiguousarray(parent.edge_off[self.idx], np.int64)
+        self.total_nindex, self.total_edges = parent.total_nindex, parent.total_edges
+
+    def struct(self, d_nindex=None, d_nlist=None, d_eweight=None):
+        """The view as an ecl_batch; device pointers default to a DeviceBatch parent's."""
+        d_nindex = d_nindex or getattr(self.parent, "d_nindex", None)
+        d_nlist = d_nlist or getattr(self.parent, "d_nlist", None)
+        d_eweight = d_eweight or getattr(self.parent, "d_eweight", None)
+        return EclBatchC(self.num_graphs, _ptr(self.nodes), _ptr(self.edges), _ptr(self.nindex_off),
+                         _ptr(self.edge_off), d_nindex, d_nlist, d_eweight)
+
+    def slice(self, inmst, k):
+        """Graph k of the view's inMST entries in a full-size output buffer."""
+        return self.parent.slice(inmst, int(self.idx[k]))
 
 
 class BatchContext:

@@ -113,3 +113,34 @@ def test_batch_learned_schedule_on_large_graphs():
         E.gen_grid(700, 700, 4103, 1 << 20), E.gen_rgg2d(400_000, 3, 4104, 1 << 20)]
     sts = _run(graphs, 1 << 16, [E.make_opts(mode=E.THRESH_LEARNED)])
     assert all(s["graphs_large"] >= 4 and s["status"] == 0 for s in sts)
+
+
+def test_shard_views_of_a_device_batch_solve_like_the_whole_batch():
+    """Each rank of a multi-GPU batch run solves a view of its shard of the
+    device-drawn batch (DeviceBatch.select): the shard's graphs get the whole
+    batch's answer at the same offsets, and no other entry is written."""
+    import shard as S
+    import torch
+    db = E.DeviceBatch(48, nmin=200, nmax=200_000)
+    out_all = torch.zeros(db.total_edges, dtype=torch.uint8, device="cuda:0")
+    bc = E.BatchContext(db.num_graphs, int(db.nodes.max()), int(db.edges.max()), 1 << 14)
+    bc.run(db, db.d_nindex, db.d_nlist, db.d_eweight, out_all.data_ptr())
+    want = out_all.cpu().numpy()
+    bc.close()
+    for gi in (0, 7, 47):  # spot checks against the oracle
+        g = db.graph(gi)
+        t, f = E.heuristic_threshold(g) if g.edges else (2**31 - 1, 0)
+        assert np.array_equal(db.slice(want, gi), O.oracle_mst(g.nindex, g.nlist, g.eweight, t, f)[0])
+    for mine in S.partition_by_cost([int(x) for x in db.edges], 3):
+        v = db.select(mine)
+        out = torch.full((db.total_edges,), 3, dtype=torch.uint8, device="cuda:0")
+        bcv = E.BatchContext(v.num_graphs, int(v.nodes.max()), int(v.edges.max()), 1 << 14)
+        for rep in range(2):  # the second run replays the captured sequence
+            bcv.run(v, None, None, None, out.data_ptr())
+            got = out.cpu().numpy()
+            for k, gi in enumerate(mine):
+                assert np.array_equal(v.slice(got, k), db.slice(want, gi)), (gi, rep)
+            for gi in set(range(db.num_graphs)) - set(mine):  # other ranks' graphs: untouched
+                assert (db.slice(got, gi) == 3).all(), (gi, rep)
+        bcv.close()
+    db.close()

@@ -69,3 +69,26 @@ def test_gather_over_gloo_world_2(tmp_path):
         g, _ = E.gen_batch_graph(int(gid), nmin=200, nmax=3000)
         _, w1, fe1 = O.oracle_mst(g.nindex, g.nlist, g.eweight)
         assert (w, fe) == (int(w1), int(fe1))
+
+
+def test_batch_view_of_a_shard_addresses_the_parent_layout():
+    """A rank's shard as a view of the packed batch: the per-graph tables are
+    the parent's rows in shard order, the entries and the output offsets stay
+    the parent's, and the ecl_batch struct carries the view's tables."""
+    import ecl_mst as E
+    graphs = [E.gen_batch_graph(i, nmin=200, nmax=3000)[0] for i in range(10)]
+    b = E.Batch(graphs)
+    for world in (2, 3):
+        for rank, mine in enumerate(S.partition_by_cost([g.edges for g in graphs], world)):
+            v = b.select(mine)
+            assert v.num_graphs == len(mine) and v.total_edges == b.total_edges
+            for k, gid in enumerate(mine):
+                assert (v.nodes[k], v.edges[k]) == (graphs[gid].nodes, graphs[gid].edges)
+                assert (v.nindex_off[k], v.edge_off[k]) == (b.nindex_off[gid], b.edge_off[gid])
+                a = int(b.edge_off[gid])
+                assert np.array_equal(b.nlist[a:a + graphs[gid].edges], graphs[gid].nlist)
+            out = np.arange(b.total_edges, dtype=np.int64)
+            assert all(np.array_equal(v.slice(out, k), b.slice(out, gid)) for k, gid in enumerate(mine))
+            st = v.struct(1, 2, 3)
+            assert st.num_graphs == len(mine) and (st.nindex, st.nlist, st.eweight) == (1, 2, 3)
+            assert st.edge_off == v.edge_off.ctypes.data
