@@ -15,7 +15,7 @@
    16 -> 64 -> 64 -> 2 MLP with the library's CUDA training kernel (Adam, one
    launch) on standardised features, graphs weighted by their solve time.
 4. Evaluate on the held-out seeds: the sweep time at the predicted setting
-   against the reference heuristic (its fallback and judge) and the best of
+   against the reference heuristic (its fallback and yardstick) and the best of
    the sweep, per family; then re-solve every held-out graph with the trained
    weights loaded, learned against heuristic, and report the measured gain
    and the share of graphs that are not slower.
