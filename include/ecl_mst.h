@@ -47,7 +47,7 @@ typedef enum ecl_status {
   ECL_ERR_OVERFLOW = -7,    /* a worklist or batch exceeded its capacity        */
   ECL_ERR_TIMEOUT = -8,     /* a device-side wait hit its limit (no hang)        */
   ECL_ERR_TOO_LARGE = -9,   /* input beyond a stated maximum                     */
-  ECL_ERR_UNSUPPORTED = -10 /* option not available in this build / device      */
+  ECL_ERR_UNSUPPORTED = -10 /* option not supported by the library or device    */
 } ecl_status;
 
 /* Human-readable name of a status code (static string). */
